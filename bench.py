@@ -1,0 +1,457 @@
+"""Benchmark of the LJ grid hot path on the 256-framework batch workload.
+
+Workload (one "step"): grids of 256 seeded triclinic frameworks (a, b, c in
+[8, 40] A, angles in [60, 120] deg, 100-5000 atoms log-uniform capped at 0.16
+atoms/A^3, 8 atom types, probes CH4 / Xe / Kr, grid spacing 0.1-0.2 A, cutoff
+12.5 A) computed by one persistent launch over a device work queue replayed
+as a CUDA graph. Data are synthetic (no dataset ships with the reference).
+
+value   pair terms/s of the batched launch, inputs resident, device-timed with
+        CUDA events on the library's stream (in-cutoff pair terms counted
+        exactly by the same traversal in counting mode, outside the timing)
+e2e     the same metric through the C ABI with host buffers: per step every
+        framework is uploaded (host preparation + H2D), the batch runs, and
+        every grid is copied back to pinned host memory
+roofline pair terms/s x 11 FP32-pipe instructions per pair against the
+        device's FP32 FMA issue rate measured by er_probe_fp32_rate
+cpu_baseline the reference's own ComputeGridSheet (oracle/_ref) on a bounded
+        sample of the same grids, on all host cores
+
+`--impl reference` times only the reference's CPU implementation.
+Multi-GPU (torchrun): every rank runs its own 256-framework batch (weak
+scaling, no collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LJ pair terms/s & Widom insertions/s; served p50/p99 vs plain, same B200"
+PAIR_INSTR = 11  # FP32-pipe instructions credited per in-cutoff pair term
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(v, pg):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, pg):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"er_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(rank):
+    from emptyroom_b200 import synth
+    return synth.config2(n_frameworks=256, seed=1000 + 100000 * rank)
+
+
+def upload_all(ctx, fws):
+    return [ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
+
+
+def count_pairs(ctx, ups, fws):
+    """Exact in-cutoff pair terms per framework (counting traversal)."""
+    import torch
+    counts = []
+    for u, f in zip(ups, fws):
+        buf = torch.empty(f.dims, dtype=torch.float32, device="cuda")
+        ctx.count_pairs_device(u, f.dims, buf.data_ptr())
+        ctx.synchronize()
+        counts.append(int(buf.double().sum().item()))
+        del buf
+    return counts
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)
+
+
+def time_plan(ctx, plan, steps, warmup, l2buf):
+    import torch
+    s = torch.cuda.ExternalStream(ctx.stream_ptr)
+    for _ in range(warmup):
+        plan.run()
+    ctx.synchronize()
+    times = []
+    for _ in range(steps):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        plan.run()
+        e1.record(s)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+    return times
+
+
+def cpu_baseline(fws, counts_fn, target_s=12.0):
+    """The reference's ComputeGridSheet on whole x-sheets of a few frameworks,
+    all host cores; returns pair terms/s on that sample."""
+    import oracle
+    cores = os.cpu_count() or 1
+    use_ref = oracle.ref_available()
+    rng = np.random.default_rng(7)
+    order = rng.permutation(len(fws))
+    done_pairs = 0.0
+    done_s = 0.0
+    sample = []
+    for k in order:
+        f = fws[int(k)]
+        nx = f.dims[0]
+        sh = [int(rng.integers(0, nx))]
+        P = f.particles()
+        t0 = time.perf_counter()
+        if use_ref:
+            oracle.ref_grid_sheets(P, f.t_matrix, f.rep, f.rc2, f.dims, sh, n_threads=cores)
+        else:
+            ny, nz = f.dims[1], f.dims[2]
+            jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+            pts = np.stack([np.full(jj.size, sh[0] / (nx - 1)), jj.ravel() / (ny - 1),
+                            kk.ravel() / (nz - 1)], -1)
+            oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
+        dt = time.perf_counter() - t0
+        done_pairs += counts_fn(int(k), sh[0])
+        done_s += dt
+        sample.append(f"fw{int(k)}:x{sh[0]}")
+        if done_s >= target_s:
+            break
+    return {"value": done_pairs / done_s, "unit": "pair-terms/s", "cores": cores,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"{len(sample)} whole x-sheets of {len(sample)} frameworks of the batch "
+                      f"({done_pairs:.3g} pair terms in {done_s:.1f} s)"}
+
+
+def run_ours(args, ws, rank, local, pg):
+    import torch
+
+    import emptyroom_b200 as er
+    torch.cuda.set_device(local)
+    ctx = er.Context(local)
+    fws = make_workload(rank)
+    ups = upload_all(ctx, fws)
+    counts = count_pairs(ctx, ups, fws)
+    pairs_step = float(sum(counts))
+    points_step = float(sum(int(np.prod(f.dims)) for f in fws))
+    outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    jobs = [(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)]
+    plan = ctx.batch_plan(jobs, er.ER_BATCH_PERSISTENT)
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    fp32_rate = ctx.fp32_rate(0.2)
+
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = time_plan(ctx, plan, args.steps, args.warmup, l2buf)
+    clk = clocks.stop()
+    barrier(pg)
+    t_step = max_over_ranks(sum(times) / len(times), pg)
+    total_pairs = sum_over_ranks(pairs_step, pg)
+    value = total_pairs / t_step
+
+    # plain per-framework launches (same grids, one launch per framework, graph-replayed)
+    plain = ctx.batch_plan(jobs, er.ER_BATCH_PLAIN)
+    ptimes = time_plan(ctx, plain, max(2, args.steps // 2), 1, l2buf)
+    t_plain = max_over_ranks(sum(ptimes) / len(ptimes), pg)
+    plain_value = total_pairs / t_plain
+    plain_launches = plain.launches
+    plain.close()
+
+    # e2e through the C ABI with host buffers
+    ref_outs = [o.cpu().numpy().copy() for o in outs[:2]]
+    host = torch.empty(int(points_step), dtype=torch.float32, pin_memory=True)
+    offs = np.cumsum([0] + [int(np.prod(f.dims)) for f in fws])
+    for u in ups:
+        u.release()
+    plan.close()
+    e2e_times = []
+    h2d = d2h = 0
+    for step in range(args.warmup + args.steps):
+        barrier(pg)
+        t0 = time.perf_counter()
+        ups2 = upload_all(ctx, fws)
+        host_jobs = [(u, f.dims, host.data_ptr() + 4 * int(offs[k]))
+                     for k, (u, f) in enumerate(zip(ups2, fws))]
+        ctx.grid_batch(host_jobs, er.ER_BATCH_PERSISTENT | er.ER_BATCH_HOST_OUT)
+        dt = time.perf_counter() - t0
+        if step == 0:
+            h2d = sum(u.device_bytes for u in ups2)
+            d2h = int(points_step) * 4
+            hv = host.numpy()
+            for k in range(2):
+                assert np.array_equal(hv[offs[k]:offs[k + 1]].reshape(fws[k].dims), ref_outs[k])
+        for u in ups2:
+            u.release()
+        if step >= args.warmup:
+            e2e_times.append(dt)
+    t_e2e = max_over_ranks(sum(e2e_times) / len(e2e_times), pg)
+
+    # roofline of the dominant (persistent) kernel
+    achieved = pairs_step * PAIR_INSTR / (sum(times) / len(times))
+    roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fp32_rate / 1e12,
+            "unit": "Tinst/s", "frac": achieved / fp32_rate,
+            "peak_source": "measured FP32 FFMA issue rate (er_probe_fp32_rate) on this GPU",
+            "traffic": load_traffic(pairs_step)}
+    line = {
+        "metric": METRIC, "value": value, "unit": "pair-terms/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded frameworks; no dataset ships with the reference)",
+        "config": {"workload": "256-framework batched LJ grids (config 2)", "frameworks": 256,
+                   "grid_points_per_step": int(points_step), "pair_terms_per_step": int(pairs_step),
+                   "cutoff_A": 12.5, "spacing_A": [0.1, 0.2],
+                   "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+        "e2e": {"value": total_pairs / t_e2e, "unit": "pair-terms/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": t_e2e * 1e3},
+        "gpu_launches": args.steps * 1,
+        "roofline": roof,
+        "clocks": clk,
+        "plain": {"value": plain_value, "unit": "pair-terms/s", "launches_per_step": plain_launches,
+                  "batched_over_plain": value / plain_value},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        starts = np.cumsum([0] + [int(np.prod(f.dims)) for f in fws])
+
+        def sheet_pairs(k, i):
+            f = fws[k]
+            u = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+            c = ctx.count_pairs(u, f.dims)
+            u.release()
+            return float(c[i].astype(np.float64).sum())
+
+        line["cpu_baseline"] = cpu_baseline(fws, sheet_pairs)
+    ctx.close()
+    return line
+
+
+def load_traffic(pairs_step):
+    """DRAM bytes per launch of the persistent kernel from the committed ncu
+    summary (profiles/grid_persistent_traffic.json), scaled by pair terms."""
+    p = os.path.join(ROOT, "profiles", "grid_persistent_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d["dram_bytes_per_pair"] * pairs_step
+
+
+def run_reference(args, ws, rank):
+    """The reference's own CPU implementation (ComputeGridSheet compiled from
+    its sources, oracle/_ref) on a bounded sample of the same workload."""
+    import oracle
+    if rank != 0:
+        return None
+    fws = make_workload(0)
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(11)
+    step_target = 3.0
+    values = []
+    samples = []
+    use_ref = oracle.ref_available()
+    for step in range(args.warmup + args.steps):
+        pairs = 0.0
+        t = 0.0
+        while t < step_target:
+            k = int(rng.integers(0, len(fws)))
+            f = fws[k]
+            P = f.particles()
+            i = int(rng.integers(0, f.dims[0]))
+            t0 = time.perf_counter()
+            if use_ref:
+                oracle.ref_grid_sheets(P, f.t_matrix, f.rep, f.rc2, f.dims, [i], n_threads=cores)
+            else:
+                ny, nz = f.dims[1], f.dims[2]
+                jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+                pts = np.stack([np.full(jj.size, i / (f.dims[0] - 1)), jj.ravel() / (ny - 1),
+                                kk.ravel() / (nz - 1)], -1)
+                oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
+            t += time.perf_counter() - t0
+            ny, nz = f.dims[1], f.dims[2]
+            jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+            pts = np.stack([np.full(jj.size, i / (f.dims[0] - 1)), jj.ravel() / (ny - 1),
+                            kk.ravel() / (nz - 1)], -1)
+            pairs += oracle.points_pairs(P, f.t_matrix, f.rep, f.rc2, pts,
+                                         n_threads=cores).sum()
+            if step == 0:
+                samples.append(f"fw{k}:x{i}")
+        if step >= args.warmup:
+            values.append(pairs / t)
+    v = float(np.mean(values))
+    kind = "reference" if use_ref else "port"
+    return {"metric": METRIC, "value": v, "unit": "pair-terms/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_target * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (seeded frameworks)", "impl": "reference",
+            "config": {"workload": "256-framework batched LJ grids (config 2)",
+                       "sample": "whole x-sheets of randomly chosen frameworks, ~3 s per step"},
+            "cpu_baseline": {"value": v, "unit": "pair-terms/s", "cores": cores, "kind": kind,
+                             "sample": f"x-sheets {samples[:8]}..., ~{step_target:.0f} s per step"},
+            "e2e": {"value": v, "unit": "pair-terms/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_case(args):
+    """Single-kernel cases for profiling: `config3` runs the 4096-atom triclinic
+    cell on a dims^3 grid (one er_grid launch per step); `widom` runs er_henry
+    with --insertions points on a config-1 cell."""
+    import torch
+
+    import emptyroom_b200 as er
+    from emptyroom_b200 import synth
+    ctx = er.Context(0)
+    if args.case == "config3":
+        f = synth.config3()
+        fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+        dims = (args.dims,) * 3
+        out = torch.empty(dims, dtype=torch.float32, device="cuda")
+        s = torch.cuda.ExternalStream(ctx.stream_ptr)
+        times = []
+        for k in range(args.warmup + args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            ctx.grid_device(fw, dims, out.data_ptr())
+            e1.record(s)
+            e1.synchronize()
+            if k >= args.warmup:
+                times.append(e0.elapsed_time(e1) * 1e-3)
+        cnt = torch.empty(dims, dtype=torch.float32, device="cuda")
+        ctx.count_pairs_device(fw, dims, cnt.data_ptr())
+        ctx.synchronize()
+        pairs = float(cnt.double().sum().item())
+        t = sum(times) / len(times)
+        print(json.dumps({"case": "config3", "dims": dims, "ms": t * 1e3, "pairs": pairs,
+                          "pair_terms_per_s": pairs / t,
+                          "pairs_per_point": pairs / float(np.prod(dims))}))
+    else:
+        f = synth.make_framework(0, (25.8, 25.8, 25.8), (90, 90, 90), 424, probe="Xe")
+        fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+        times = []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            r = ctx.henry(fw, 298.0, args.insertions, seed=k)
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        t = sum(times) / len(times)
+        print(json.dumps({"case": "widom", "insertions": args.insertions, "ms": t * 1e3,
+                          "insertions_per_s": args.insertions / t, "kh": r["kh_mol_m3_pa"]}))
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", default="batch", choices=["batch", "config3", "widom"])
+    ap.add_argument("--dims", type=int, default=256)
+    ap.add_argument("--insertions", type=int, default=10_000_000)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.case != "batch":
+        run_case(args)
+        return
+    ws, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        line = run_reference(args, ws, rank)
+    else:
+        line = run_ours(args, ws, rank, local, pg)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

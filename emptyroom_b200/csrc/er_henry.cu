@@ -1,0 +1,309 @@
+// er_henry.cu -- Widom insertions and the Henry coefficient (er_henry).
+//
+// Replaces doHenry (src/doHenry.h:29-135) and its host reduction
+// (src/henry.cu:157-174). Pipeline, all on the context stream:
+//   1. gen     insertion i -> Philox4x32-10 point (stream `seed`), pocket-mask
+//              test, spatial bin key (bins of ~16 expected points, 2x2x2 bricks)
+//   2. scan    bin counts -> bin starts
+//   3. scatter insertion indices into their bins; 4. sort each bin ascending
+//      (so the layout, and with it every FP32 rounding, is deterministic)
+//   5. energy  the shared LJ engine over 1024 sorted points per CTA
+//   6. reduce  FP64 log-sum-exp of exp(-E/T) and E exp(-E/T) in insertion
+//              order with a fixed tree: (m, s, se) with sum w = s e^m.
+#include <math.h>
+
+#include <algorithm>
+
+#include "er_ctx.h"
+#include "er_engine.cuh"
+#include "er_philox.h"
+
+namespace er {
+
+struct BinGeom {
+    int nb[3];  // bins per fractional axis
+    int NB[3];  // 2x2x2 bricks per axis
+    int n_keys;
+};
+
+struct Lse {
+    double m, s, se;
+};
+
+__device__ __forceinline__ int bin_key(const double* f, const BinGeom& g) {
+    int b[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) b[d] = min(g.nb[d] - 1, max(0, (int)(f[d] * g.nb[d])));
+    return (((b[0] >> 1) * g.NB[1] + (b[1] >> 1)) * g.NB[2] + (b[2] >> 1)) * 8 +
+           ((b[0] & 1) << 2) + ((b[1] & 1) << 1) + (b[2] & 1);
+}
+
+// Corner test of the pocket mask; the cell lookup follows src/gcmc.cc:155-157.
+__device__ __forceinline__ bool blocked_at(const uint8_t* mask, int nx, int ny, int nz,
+                                           const double* p) {
+    const double dxf = __ddiv_rn(1.0, (double)(nx - 1));
+    const double dyf = __ddiv_rn(1.0, (double)(ny - 1));
+    const double dzf = __ddiv_rn(1.0, (double)(nz - 1));
+    const int i0 = min((int)floor(__ddiv_rn(p[0], dxf)), nx - 2);
+    const int j0 = min((int)floor(__ddiv_rn(p[1], dyf)), ny - 2);
+    const int k0 = min((int)floor(__ddiv_rn(p[2], dzf)), nz - 2);
+    for (int di = 0; di < 2; ++di)
+        for (int dj = 0; dj < 2; ++dj)
+            for (int dk = 0; dk < 2; ++dk) {
+                const size_t idx = (size_t)(k0 + dk) + (size_t)(j0 + dj) * nz +
+                                   (size_t)(i0 + di) * ny * nz;
+                if (mask[idx]) return true;
+            }
+    return false;
+}
+
+__global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t* __restrict__ mask,
+                                 int mnx, int mny, int mnz, double* __restrict__ pts,
+                                 int* __restrict__ key, int* __restrict__ counts,
+                                 float* __restrict__ energies, int* __restrict__ n_blocked) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double f[3];
+        insertion_point(seed, (uint64_t)i, f);
+        pts[3 * (size_t)i] = f[0];
+        pts[3 * (size_t)i + 1] = f[1];
+        pts[3 * (size_t)i + 2] = f[2];
+        if (mask && blocked_at(mask, mnx, mny, mnz, f)) {
+            key[i] = -1;
+            energies[i] = INFINITY;
+            atomicAdd(n_blocked, 1);
+        } else {
+            const int k = bin_key(f, g);
+            key[i] = k;
+            atomicAdd(&counts[k], 1);
+        }
+    }
+}
+
+// Exclusive scan of n ints by one CTA of 1024 threads (contiguous chunks);
+// out[n] receives the total.
+__global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ in,
+                                                    int* __restrict__ out, int n) {
+    __shared__ int sums[1024];
+    const int t = threadIdx.x;
+    const int per = (n + 1023) / 1024;
+    const int lo = min(n, t * per), hi = min(n, lo + per);
+    int s = 0;
+    for (int i = lo; i < hi; ++i) s += in[i];
+    sums[t] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int v = t >= o ? sums[t - o] : 0;
+        __syncthreads();
+        sums[t] += v;
+        __syncthreads();
+    }
+    int run = sums[t] - s;
+    for (int i = lo; i < hi; ++i) {
+        const int v = in[i];
+        out[i] = run;
+        run += v;
+    }
+    if (t == 1023) out[n] = sums[1023];
+}
+
+__global__ void henry_scatter_kernel(const int* __restrict__ key, int n,
+                                     const int* __restrict__ starts, int* __restrict__ fill,
+                                     int* __restrict__ tmp) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k = key[i];
+        if (k >= 0) tmp[starts[k] + atomicAdd(&fill[k], 1)] = i;
+    }
+}
+
+// One warp per bin: rank of each entry among its bin's entries -> ascending order.
+__global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_keys,
+                                       const int* __restrict__ tmp, int* __restrict__ order) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n_keys; b += warps) {
+        const int s = starts[b], L = starts[b + 1] - s;
+        for (int q = lane; q < L; q += 32) {
+            const int v = tmp[s + q];
+            int rank = 0;
+            for (int r = 0; r < L; ++r) rank += tmp[s + r] < v;
+            order[s + rank] = v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+    henry_energy_kernel(const __grid_constant__ PointTask task) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if ((long long)blockIdx.x * (kWarps * 32 * kP) >= (long long)*task.n_valid) return;
+    EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
+    PointPolicy pol(&task, blockIdx.x);
+    process_cta<PointPolicy, PREC_COMP>(s, pol, task.fw, task.cc);
+}
+
+__device__ __forceinline__ Lse lse_merge(Lse a, Lse b) {
+    if (b.s == 0.0) return a;
+    if (a.s == 0.0) return b;
+    const double M = fmax(a.m, b.m);
+    const double fa = exp(a.m - M), fb = exp(b.m - M);
+    return Lse{M, a.s * fa + b.s * fb, a.se * fa + b.se * fb};
+}
+
+__device__ __forceinline__ Lse lse_tree(Lse v, Lse* sm) {
+    const int t = threadIdx.x;
+    sm[t] = v;
+    __syncthreads();
+    for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+        if (t < o) sm[t] = lse_merge(sm[t], sm[t + o]);
+        __syncthreads();
+    }
+    return sm[0];
+}
+
+// Block b sums insertions [b*chunk, (b+1)*chunk) (thread t: b*chunk + t + 256 k).
+__global__ void __launch_bounds__(256) henry_reduce_kernel(const float* __restrict__ E, int n,
+                                                           double T, int chunk,
+                                                           Lse* __restrict__ part) {
+    __shared__ Lse sm[256];
+    const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    Lse acc{-INFINITY, 0.0, 0.0};
+    for (int i = lo + threadIdx.x; i < hi; i += 256) {
+        const float ef = E[i];
+        if (isinf(ef)) continue;  // blocked insertion: weight 0
+        const double e = (double)ef;
+        const double x = -e / T;  // src/doHenry.h:107, exp(-energy / T)
+        if (x > acc.m) {
+            const double f = exp(acc.m - x);
+            acc.s = acc.s * f + 1.0;
+            acc.se = acc.se * f + e;
+            acc.m = x;
+        } else {
+            const double w = exp(x - acc.m);
+            acc.s += w;
+            acc.se += e * w;
+        }
+    }
+    const Lse r = lse_tree(acc, sm);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(256) henry_final_kernel(const Lse* __restrict__ part, int nb,
+                                                          Lse* __restrict__ out) {
+    __shared__ Lse sm[256];
+    Lse acc{-INFINITY, 0.0, 0.0};
+    for (int i = threadIdx.x; i < nb; i += 256) acc = lse_merge(acc, part[i]);
+    const Lse r = lse_tree(acc, sm);
+    if (threadIdx.x == 0) *out = r;
+}
+
+}  // namespace er
+
+using namespace er;
+
+extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
+                        const uint8_t* block_mask, int mnx, int mny, int mnz,
+                        er_henry_result* out, float* energies_out) {
+    if (!ctx || !out) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    const FwRecord* f = find_fw(ctx, fw_id);
+    if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "henry: unknown framework id");
+    if (!(temperature > 0.0) || !std::isfinite(temperature))
+        return set_error(ctx, ER_ERR_INVALID, "henry: temperature must be positive");
+    if (n_ins < 1) return set_error(ctx, ER_ERR_INVALID, "henry: n_ins must be >= 1");
+    if (n_ins > (int64_t)INT32_MAX - 4096)
+        return set_error(ctx, ER_ERR_LIMIT, "henry: more than 2^31 - 4097 insertions per call");
+    if (block_mask && (mnx < 2 || mny < 2 || mnz < 2))
+        return set_error(ctx, ER_ERR_INVALID, "henry: mask dims must be >= 2");
+    const int n = (int)n_ins;
+    // bins of ~16 expected points, shaped after the cell vector lengths
+    BinGeom g;
+    {
+        const double L0 = f->cell_len[0], L1 = f->cell_len[1], L2 = f->cell_len[2];
+        const double scale = cbrt((double)n / 16.0 / (L0 * L1 * L2));
+        const double L[3] = {L0, L1, L2};
+        int64_t nk = 8;
+        for (int d = 0; d < 3; ++d) {
+            g.nb[d] = (int)std::min<double>(2048.0, std::max(1.0, floor(L[d] * scale + 0.5)));
+            g.NB[d] = (g.nb[d] + 1) / 2;
+            nk *= g.NB[d];
+        }
+        if (nk > (int64_t)256 * 1024 * 1024)
+            return set_error(ctx, ER_ERR_LIMIT, "henry: bin table too large");
+        g.n_keys = (int)nk;
+    }
+    const size_t N = (size_t)n;
+    if (ctx->h_pts.ensure(3 * N * sizeof(double)) || ctx->h_bin.ensure(N * sizeof(int)) ||
+        ctx->h_order.ensure(N * sizeof(int)) || ctx->h_tmp.ensure(N * sizeof(int)) ||
+        ctx->h_counts.ensure(2 * (size_t)g.n_keys * sizeof(int)) ||
+        ctx->h_starts.ensure(((size_t)g.n_keys + 1) * sizeof(int)) ||
+        ctx->h_e.ensure(N * sizeof(float)) || ctx->h_nwt.ensure(4 * sizeof(int)) ||
+        ctx->h_part.ensure(4096 * sizeof(Lse)) || ctx->h_res.ensure(sizeof(Lse)))
+        return set_error(ctx, ER_ERR_NOMEM, "henry: device scratch allocation failed");
+    const uint8_t* d_mask = nullptr;
+    if (block_mask) {
+        const size_t mb = (size_t)mnx * mny * mnz;
+        if (ctx->h_mask.ensure(mb)) return set_error(ctx, ER_ERR_NOMEM, "henry: mask allocation");
+        ER_CUDA(ctx, cudaMemcpyAsync(ctx->h_mask.ptr, block_mask, mb, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        d_mask = (const uint8_t*)ctx->h_mask.ptr;
+    }
+    int* counts = (int*)ctx->h_counts.ptr;
+    int* fill = counts + g.n_keys;
+    int* starts = (int*)ctx->h_starts.ptr;
+    int* nblk = (int*)ctx->h_nwt.ptr;
+    float* E = (float*)ctx->h_e.ptr;
+    cudaStream_t st = ctx->stream;
+    ER_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * (size_t)g.n_keys * sizeof(int), st));
+    ER_CUDA(ctx, cudaMemsetAsync(nblk, 0, sizeof(int), st));
+    const int gthreads = 256;
+    const int gblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads,
+                                               (int64_t)ctx->num_sms * 32);
+    henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
+                                                   (double*)ctx->h_pts.ptr, (int*)ctx->h_bin.ptr,
+                                                   counts, E, nblk);
+    scan_kernel<<<1, 1024, 0, st>>>(counts, starts, g.n_keys);
+    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)ctx->h_bin.ptr, n, starts,
+                                                       fill, (int*)ctx->h_tmp.ptr);
+    henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
+                                                              (const int*)ctx->h_tmp.ptr,
+                                                              (int*)ctx->h_order.ptr);
+    ER_CUDA(ctx, cudaGetLastError());
+    PointTask task;
+    task.fw = f->dev;
+    task.cc = make_cutoff_consts(f->rc2, 0.0, 1e-16 * 1e-16);  // min_r, src/doHenry.h:15
+    task.pts = (const double*)ctx->h_pts.ptr;
+    task.order = (const int*)ctx->h_order.ptr;
+    task.n_valid = starts + g.n_keys;
+    task.energies = E;
+    ER_CUDA(ctx, cudaFuncSetAttribute(henry_energy_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(EngineSmem)));
+    const int per_cta = kWarps * 32 * kP;
+    const int ecta = (n + per_cta - 1) / per_cta;
+    henry_energy_kernel<<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
+    ER_CUDA(ctx, cudaGetLastError());
+    const int rblocks = std::min(4096, std::max(1, ctx->num_sms * 4));
+    const int chunk = (n + rblocks - 1) / rblocks;
+    const int nrb = (n + chunk - 1) / chunk;
+    henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, temperature, chunk, (Lse*)ctx->h_part.ptr);
+    henry_final_kernel<<<1, 256, 0, st>>>((const Lse*)ctx->h_part.ptr, nrb, (Lse*)ctx->h_res.ptr);
+    ER_CUDA(ctx, cudaGetLastError());
+    Lse r;
+    int nb_host = 0;
+    ER_CUDA(ctx, cudaMemcpyAsync(&r, ctx->h_res.ptr, sizeof(Lse), cudaMemcpyDeviceToHost, st));
+    ER_CUDA(ctx, cudaMemcpyAsync(&nb_host, nblk, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (energies_out)
+        ER_CUDA(ctx, cudaMemcpyAsync(energies_out, E, N * sizeof(float), cudaMemcpyDeviceToHost,
+                                     st));
+    ER_CUDA(ctx, cudaStreamSynchronize(st));
+    out->log_scale = r.m;
+    out->sum_w_scaled = r.s;
+    out->sum_ew_scaled = r.se;
+    out->sum_w = r.s > 0 ? r.s * exp(r.m) : 0.0;
+    out->sum_ew = r.s > 0 ? r.se * exp(r.m) : 0.0;
+    out->n_insertions = (double)n;
+    out->n_blocked = (double)nb_host;
+    out->mean_energy = r.s > 0 ? r.se / r.s : 0.0;
+    // K_H = sum w / N / T / 8.314 (mol/(m^3 Pa)), src/henry.cu:169
+    out->kh_mol_m3_pa = out->sum_w / (double)n / temperature / 8.314;
+    return ER_OK;
+}

@@ -1,0 +1,216 @@
+/*
+ * emptyroom_b200.h -- C ABI of the B200 (sm_100a) adsorption hot path.
+ *
+ * One shared library, libemptyroom_b200.so, replaces the device-compute seam of
+ * CorySimon/EmptyRoom: the kernel launches in src/writegrid.cu and src/henry.cu
+ * and the CPU flood fill of src/pocketblocking.cc. Signatures use plain C
+ * types only. Every call returns an er_status (ER_OK == 0) and never exits the
+ * process; er_ctx_last_error() describes the last failure of a context.
+ * A context is used by one host thread at a time; contexts are independent.
+ * Host buffers stay owned by the caller.
+ */
+#ifndef EMPTYROOM_B200_H_
+#define EMPTYROOM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    ER_OK = 0,
+    ER_ERR_INVALID = 1,   /* bad argument (sizes, ids, NULL) */
+    ER_ERR_CUDA = 2,      /* CUDA runtime error or no usable device */
+    ER_ERR_NOMEM = 3,     /* device or host allocation failed / over budget */
+    ER_ERR_IO = 4,        /* file could not be read or written */
+    ER_ERR_NOT_FOUND = 5, /* label / id not found */
+    ER_ERR_TIMEOUT = 6,   /* a bounded wait ran out */
+    ER_ERR_LIMIT = 7      /* a documented size limit was exceeded */
+} er_status;
+
+const char* er_status_string(int status);
+
+/* ------------------------------------------------------------------ types */
+/* Same field order and meaning as FrameworkParticle (src/datatypes.h:20-28):
+ * fractional position and the Lorentz-Berthelot mixed epsilon (K) and
+ * sigma^2 (A^2) of this framework atom with the probe. */
+typedef struct {
+    double x_f, y_f, z_f;
+    double eps_with_adsorbate;
+    double sig_with_adsorbate_squared;
+} er_particle;
+
+/* What the reference passes to its kernels by value in GridParameters /
+ * HenryParameters (src/datatypes.h:44-110): the atoms, the fractional ->
+ * Cartesian matrix (row-major, src/Framework.cc:124-132), the unit-cell
+ * replication factors (images -rep..rep per axis) and the squared cutoff. */
+typedef struct {
+    int n_atoms;
+    const er_particle* atoms; /* host pointer, n_atoms entries */
+    double t_matrix[9];
+    int rep[3];
+    double r_cutoff_squared;
+} er_framework_desc;
+
+typedef struct er_ctx er_ctx;
+
+/* ------------------------------------------------------------------ context */
+/* Binds `device`, creates the context's stream and allocator. */
+int er_ctx_create(int device, er_ctx** out);
+void er_ctx_destroy(er_ctx* ctx);
+const char* er_ctx_last_error(const er_ctx* ctx);
+/* Waits for all work queued on the context's stream. */
+int er_ctx_synchronize(er_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the library's launches. */
+int er_ctx_stream(er_ctx* ctx, void** stream);
+
+/* ------------------------------------------------------------------ frameworks */
+/* Uploads a framework/probe pair and builds its device-resident image cell
+ * list. Replaces the cudaMalloc/cudaMemcpy of FrameworkParticle[] at
+ * src/writegrid.cu:187-189 and src/henry.cu:133-135. *fw_id receives a handle. */
+int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id);
+int er_framework_release(er_ctx* ctx, int fw_id);
+/* Device bytes held by a framework handle. */
+int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);
+
+/* ------------------------------------------------------------------ grids */
+/* Output placement / type / precision flags for er_grid. */
+#define ER_OUT_HOST 0x0      /* out is a host pointer (copied back inside the call) */
+#define ER_OUT_DEVICE 0x1    /* out is a device pointer on the context's device */
+#define ER_OUT_F32 0x0       /* float per point */
+#define ER_OUT_F64 0x2       /* double per point (the reference's sheet type) */
+#define ER_PREC_COMP 0x0     /* FP32 pair terms, compensated (two-float) accumulation */
+#define ER_PREC_FP32 0x10    /* FP32 pair terms, plain FP32 accumulation */
+#define ER_PREC_FP64 0x20    /* FP64 pair terms and accumulation (precision sweeps) */
+#define ER_COUNT_PAIRS 0x40  /* diagnostic: write the number of in-cutoff pair terms per
+                                point instead of the energy (same traversal) */
+
+/* Energies above this value (K) are written as this value (overflow cap). */
+#define ER_ENERGY_CAP 1.0e30
+
+/* Probe-framework LJ energy (K) at every point of an nx x ny x nz grid with
+ * fractional axes i/(N-1), endpoints included, layout out[k + j*nz + i*ny*nz]:
+ * the values ComputeGridSheet (src/computegridsheet.h:30-99) produces for all
+ * x-sheets of src/writegrid.cu:219-226. Requires nx, ny, nz >= 2. */
+int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out);
+
+/* One x = x_index sheet as double[ny*nz] on the host, index k + j*nz: the
+ * drop-in for one ComputeGridSheet launch plus its D2H copy
+ * (src/writegrid.cu:221-232). */
+int er_grid_sheet(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int x_index,
+                  double* out_sheet);
+
+/* Hard-sphere accessibility (1 accessible, 0 overlap: some image within
+ * +-1 cells has r^2 < sigma_mix^2), the ComputeGridSheetAccessibleOrNot
+ * semantics of src/computegridsheet.h:101-165, host uint8 out. */
+int er_accessibility(er_ctx* ctx, int fw_id, int nx, int ny, int nz, uint8_t* out);
+
+/* ------------------------------------------------------------------ batches */
+typedef struct {
+    int fw_id;
+    int nx, ny, nz;
+    float* out_device; /* device buffer of nx*ny*nz floats */
+} er_grid_job;
+
+#define ER_BATCH_PERSISTENT 0 /* one persistent launch over a device work queue */
+#define ER_BATCH_PLAIN 1      /* one plain launch per job, in order */
+#define ER_BATCH_HOST_OUT 0x100 /* or-ed into mode: out_device fields are host pointers;
+                                   grids are staged on the device and copied back */
+
+/* Runs many grid jobs (uneven frameworks, probes, grid sizes). Results are
+ * identical between the two modes and independent of the job mix. */
+int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode);
+
+/* A batch plan fixes the work queue once and replays it as a CUDA graph. */
+typedef struct er_batch_plan er_batch_plan;
+int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode,
+                         er_batch_plan** out);
+int er_batch_plan_run(er_batch_plan* plan); /* asynchronous on the context stream */
+/* Kernel launches one run of the plan issues (its CUDA graph's kernel nodes). */
+int er_batch_plan_launches(const er_batch_plan* plan, int* n_launches);
+void er_batch_plan_destroy(er_batch_plan* plan);
+
+/* ------------------------------------------------------------------ Widom / Henry */
+typedef struct {
+    double sum_w;           /* sum over insertions of exp(-E/T) */
+    double sum_ew;          /* sum of E exp(-E/T) (K) */
+    double log_scale;       /* m: sum_w = sum_w_scaled * exp(m) (log-sum-exp form) */
+    double sum_w_scaled;    /* sum of exp(-E/T - m) */
+    double sum_ew_scaled;   /* sum of E exp(-E/T - m) */
+    double n_insertions;    /* insertions performed (blocked ones included) */
+    double n_blocked;       /* insertions that fell in a blocked grid cell */
+    double mean_energy;     /* <E> = sum_ew / sum_w (K) */
+    double kh_mol_m3_pa;    /* K_H = sum_w / (N T 8.314), src/henry.cu:169 */
+} er_henry_result;
+
+/* Widom insertions i = 0..n_ins-1 at Philox4x32-10 points of stream `seed`
+ * (fractional coordinates uniform in [0,1), 53 bits each), E by the pair sum
+ * of src/doHenry.h:70-98, FP64 log-sum-exp reduction of
+ * src/doHenry.h:106-125 and src/henry.cu:157-169. block_mask (host, may be
+ * NULL) is an mnx x mny x mnz grid (axes i/(N-1)); an insertion whose 8
+ * surrounding corners include a set entry is blocked and has weight 0.
+ * energies_out (host, may be NULL) receives E per insertion as float. */
+int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
+             const uint8_t* block_mask, int mnx, int mny, int mnz, er_henry_result* out,
+             float* energies_out);
+
+/* ------------------------------------------------------------------ pocket blocking */
+/* FindAndBlockPockets (src/pocketblocking.cc:126-391) on the GPU: points with
+ * E >= 15 T are inaccessible; accessible points form 6-connected segments
+ * (no periodic wrap); segments linked across the periodic faces are
+ * classified CHANNEL or POCKET; pocket points are overwritten with 1e13.
+ * grid is a host double[nx*ny*nz] modified in place; *n_pockets receives the
+ * reference's return value. segments_out (host, may be NULL) receives the
+ * segment id per point (-1 inaccessible) in the reference's numbering. */
+int er_block_pockets(er_ctx* ctx, double* grid, int nx, int ny, int nz, double temperature,
+                     int* n_pockets, int* segments_out);
+
+/* Device form: grid is a device float[nx*ny*nz] (left unchanged);
+ * pocket_mask_out (device uint8[nx*ny*nz]) receives 1 at pocket points. */
+int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, int ny, int nz,
+                            double temperature, uint8_t* pocket_mask_out, int* n_pockets);
+
+/* ------------------------------------------------------------------ host helpers */
+/* Fractional -> Cartesian matrix and its inverse from cell lengths (A) and
+ * angles (degrees), the formulas of src/Framework.cc:113-142. Returns
+ * ER_ERR_INVALID for a degenerate cell. volume receives V (A^3). */
+int er_cell_matrices(double a, double b, double c, double alpha_deg, double beta_deg,
+                     double gamma_deg, double t_matrix[9], double inv_t_matrix[9],
+                     double* volume);
+
+/* Replication factors floor(rc / w_i) + 1, w_i the perpendicular cell widths:
+ * enough images that every image within rc of any grid point is summed
+ * (the .uc files read at src/readsettings.h:243-274). factor 2 gives the
+ * "twice" variant (w_i >= 2 rc per replicated cell). */
+int er_replication_factors(const double t_matrix[9], double r_cutoff, int factor, int rep[3]);
+
+/* Philox4x32-10 block (host copy of the device generator). */
+void er_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* Insertion point i of stream seed (the points er_henry uses). */
+void er_insertion_point(uint64_t seed, uint64_t i, double out[3]);
+
+/* Seeded synthetic framework: n_atoms fractional positions uniform in [0,1)
+ * with minimum periodic pair distance d_min (A, 0 disables), rejection
+ * sampled with a cell list. Returns ER_ERR_LIMIT when the density cannot
+ * be reached within the attempt budget. */
+int er_synth_positions(uint64_t seed, const double t_matrix[9], int n_atoms, double d_min,
+                       double* frac_out);
+
+/* ------------------------------------------------------------------ diagnostics */
+/* Measures the device's FP32 FMA issue rate with a chain of independent FFMAs
+ * (FP32-pipe lane-instructions per second, whole GPU) over about `seconds`.
+ * This is the denominator of the pair-sum roofline. */
+int er_probe_fp32_rate(er_ctx* ctx, double seconds, double* instr_per_s);
+
+/* Library version string. */
+const char* er_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMPTYROOM_B200_H_ */

@@ -1,0 +1,213 @@
+"""Parity of the CUDA grid path (er_grid and friends, through the C ABI) with
+the reference's FP64 results: the golden fixtures, the oracle at full grids
+of small cells, and the oracle at sampled points of large grids."""
+import numpy as np
+import pytest
+
+import emptyroom_b200 as er
+import oracle
+from conftest import golden, grid_errors
+from emptyroom_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(stats):
+    assert stats["neg_ok"], stats
+    assert stats["pos_ok"], stats
+    assert stats["cap_ok"], stats
+
+
+@pytest.mark.parametrize("name", ["grid_cubic", "grid_triclinic", "grid_rep2"])
+def test_grid_matches_golden(ctx, name):
+    g = golden(name)
+    fw = ctx.upload(g["particles"], g["t_matrix"], g["rep"], float(g["rc2"]))
+    e = ctx.grid(fw, g["dims"])
+    S = oracle.grid_abs(g["particles"], g["t_matrix"], g["rep"], float(g["rc2"]), g["dims"])
+    _check(grid_errors(e, g["grid"], S))
+    fw.release()
+
+
+def test_grid_config1_full(ctx):
+    fw_s = synth.config1(0)
+    P = fw_s.particles()
+    fw = ctx.upload(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    e = ctx.grid(fw, (32, 32, 32))
+    ref = oracle.grid(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, (32, 32, 32))
+    S = oracle.grid_abs(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, (32, 32, 32))
+    st = grid_errors(e, ref, S)
+    _check(st)
+    assert st["n_neg"] > 0
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_grid_triclinic_odd_sizes(ctx, seed):
+    rng = np.random.default_rng(seed)
+    abc = tuple(rng.uniform(9, 30, size=3))
+    ang = tuple(rng.uniform(65, 115, size=3))
+    n = int(rng.integers(20, 300))
+    fw_s = synth.make_framework(seed, abc, ang, n, probe=["CH4", "Xe", "Kr"][seed % 3])
+    dims = tuple(int(x) for x in rng.integers(2, 23, size=3))
+    P = fw_s.particles()
+    fw = ctx.upload(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    e = ctx.grid(fw, dims)
+    ref = oracle.grid(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, dims)
+    S = oracle.grid_abs(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, dims)
+    _check(grid_errors(e, ref, S))
+
+
+def test_grid_large_sampled_points(ctx):
+    """config-3 cell (4096 atoms) on a 96^3 grid: 3000 sampled points vs the oracle."""
+    fw_s = synth.config3()
+    P = fw_s.particles()
+    fw = ctx.upload(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    dims = (96, 96, 96)
+    e = ctx.grid(fw, dims)
+    rng = np.random.default_rng(0)
+    idx = rng.integers(0, np.array(dims), size=(3000, 3))
+    pts = idx / (np.array(dims) - 1.0)
+    ref = oracle.points(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, pts, 1e-12)
+    S = oracle.points_abs(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, pts, 1e-12)
+    _check(grid_errors(e[idx[:, 0], idx[:, 1], idx[:, 2]], ref, S))
+
+
+def test_sheet_and_f64_and_device_outputs_agree(ctx):
+    import torch
+    fw_s = synth.config1(3)
+    fw = ctx.upload(fw_s.particles(), fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    dims = (17, 18, 19)
+    e32 = ctx.grid(fw, dims)
+    e64 = ctx.grid(fw, dims, f64=True)
+    assert e64.dtype == np.float64 and np.array_equal(e64, e32.astype(np.float64))
+    for i in (0, 7, 16):
+        assert np.array_equal(ctx.grid_sheet(fw, dims, i), e32[i].astype(np.float64))
+    d = torch.empty(dims, dtype=torch.float32, device="cuda")
+    ctx.grid_device(fw, dims, d.data_ptr())
+    ctx.synchronize()
+    assert np.array_equal(d.cpu().numpy(), e32)
+    d64 = torch.empty(dims, dtype=torch.float64, device="cuda")
+    ctx.grid_device(fw, dims, d64.data_ptr(), f64=True)
+    ctx.synchronize()
+    assert np.array_equal(d64.cpu().numpy(), e64)
+
+
+def test_grid_is_deterministic(ctx):
+    fw_s = synth.config1(4)
+    fw = ctx.upload(fw_s.particles(), fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    a = ctx.grid(fw, (33, 31, 29))
+    b = ctx.grid(fw, (33, 31, 29))
+    assert np.array_equal(a, b)
+
+
+def test_fp32_mode_close(ctx):
+    fw_s = synth.config1(5)
+    P = fw_s.particles()
+    fw = ctx.upload(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    dims = (20, 20, 20)
+    e = ctx.grid(fw, dims, precision=er.ER_PREC_FP32)
+    ref = oracle.grid(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, dims)
+    S = oracle.grid_abs(P, fw_s.t_matrix, fw_s.rep, fw_s.rc2, dims)
+    neg = ref < 0
+    assert np.all(np.abs(e[neg] - ref[neg]) <= 1e-5 * np.abs(ref[neg]) + 1e-5 * S[neg])
+
+
+def test_invalid_arguments(ctx):
+    fw_s = synth.config1(6)
+    fw = ctx.upload(fw_s.particles(), fw_s.t_matrix, fw_s.rep, fw_s.rc2)
+    with pytest.raises(er.ErError):
+        ctx.grid(fw, (1, 8, 8))
+    with pytest.raises(er.ErError):
+        ctx.upload(fw_s.particles(), fw_s.t_matrix, fw_s.rep, -1.0)
+    bad = er.Framework(ctx, 987654, 0)
+    with pytest.raises(er.ErError):
+        ctx.grid(bad, (4, 4, 4))
+
+
+def test_empty_framework_gives_zero(ctx):
+    t, _, _ = er.cell_matrices(10, 10, 10, 90, 90, 90)
+    fw = ctx.upload(np.zeros((0, 5)), t, (1, 1, 1), 100.0)
+    e = ctx.grid(fw, (5, 5, 5))
+    assert np.all(e == 0)
+
+
+def test_point_on_atom_is_capped(ctx):
+    """A grid point exactly on an atom: the reference gives an astronomically
+    large finite value; the CUDA path writes the overflow cap."""
+    t, _, _ = er.cell_matrices(10, 10, 10, 90, 90, 90)
+    P = er.particles([[0.5, 0.5, 0.5], [0.1, 0.2, 0.3]], [50.0, 60.0], [9.0, 10.0])
+    fw = ctx.upload(P, t, (1, 1, 1), 25.0)
+    dims = (3, 3, 3)  # the centre point (1,1,1) sits on atom 0
+    e = ctx.grid(fw, dims)
+    ref = oracle.grid(P, t, (1, 1, 1), 25.0, dims)
+    assert ref[1, 1, 1] > 1e30 and e[1, 1, 1] == np.float32(1e30)
+    _check(grid_errors(e, ref, oracle.grid_abs(P, t, (1, 1, 1), 25.0, dims)))
+
+
+def _batch_frameworks(ctx, n=12, seed=50):
+    fws = synth.config2(n_frameworks=n, seed=seed, spacing_range=(0.9, 1.6))
+    ups = [ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
+    return fws, ups
+
+
+def test_batch_modes_identical_and_match_single(ctx):
+    import torch
+    fws, ups = _batch_frameworks(ctx)
+    outs_p = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    outs_q = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs_p)],
+                   er.ER_BATCH_PERSISTENT)
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs_q)],
+                   er.ER_BATCH_PLAIN)
+    for u, f, a, b in zip(ups, fws, outs_p, outs_q):
+        single = ctx.grid(u, f.dims)
+        assert np.array_equal(a.cpu().numpy(), single)
+        assert np.array_equal(b.cpu().numpy(), single)
+
+
+def test_batch_alone_equals_in_mix(ctx):
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=10, seed=77)
+    outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)])
+    k = 4
+    alone = torch.empty(fws[k].dims, dtype=torch.float32, device="cuda")
+    ctx.grid_batch([(ups[k], fws[k].dims, alone.data_ptr())])
+    assert torch.equal(alone, outs[k])
+
+
+def test_batch_plan_graph_replay(ctx):
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=6, seed=91)
+    outs = [torch.zeros(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    plan = ctx.batch_plan([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)])
+    assert plan.launches == 1
+    plan.run()
+    ctx.synchronize()
+    first = [o.clone() for o in outs]
+    for o in outs:
+        o.zero_()
+    plan.run()
+    ctx.synchronize()
+    for a, b in zip(first, outs):
+        assert torch.equal(a, b)
+    plain = ctx.batch_plan([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)],
+                           er.ER_BATCH_PLAIN)
+    assert plain.launches == len(fws)
+    plan.close()
+    plain.close()
+
+
+def test_batch_matches_oracle_sampled(ctx):
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=5, seed=123)
+    outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)])
+    rng = np.random.default_rng(1)
+    for f, o in zip(fws, outs):
+        dims = np.array(f.dims)
+        idx = rng.integers(0, dims, size=(200, 3))
+        pts = idx / (dims - 1.0)
+        ref = oracle.points(f.particles(), f.t_matrix, f.rep, f.rc2, pts, 1e-12)
+        S = oracle.points_abs(f.particles(), f.t_matrix, f.rep, f.rc2, pts, 1e-12)
+        got = o.cpu().numpy()[idx[:, 0], idx[:, 1], idx[:, 2]]
+        _check(grid_errors(got, ref, S))

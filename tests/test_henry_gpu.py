@@ -1,0 +1,103 @@
+"""Parity of the CUDA Widom path (er_henry) with the FP64 oracle fed the same
+Philox insertion points: K_H within 1e-6 relative, per-insertion energies
+within the grid tolerances, blocked-insertion counts exact."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import grid_errors
+from emptyroom_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+KH_RTOL = 1e-6
+
+
+def _fw(ctx, seed=0, n_atoms=424, probe="Xe"):
+    f = synth.make_framework(seed, (25.8, 25.8, 25.8), (90, 90, 90), n_atoms, probe=probe)
+    P = f.particles()
+    return f, P, ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+
+
+def _kh(sum_w, n, T):
+    return sum_w / n / T / 8.314
+
+
+@pytest.mark.parametrize("seed,n_ins", [(0, 100000), (1, 37777), (2, 1), (3, 257)])
+def test_henry_matches_oracle(ctx, seed, n_ins):
+    f, P, fw = _fw(ctx, seed)
+    T = 298.0
+    r = ctx.henry(fw, T, n_ins, seed=seed + 10, want_energies=True)
+    o = oracle.henry(P, f.t_matrix, f.rep, f.rc2, T, seed + 10, n_ins, want_energies=True)
+    pts = np.array([oracle.insertion_point(seed + 10, i) for i in range(min(n_ins, 3000))])
+    S = oracle.points_abs(P, f.t_matrix, f.rep, f.rc2, pts, 1e-16)
+    st = grid_errors(r["energies"][:len(pts)], o["energies"][:len(pts)], S)
+    assert st["neg_ok"] and st["pos_ok"] and st["cap_ok"], st
+    kh_o = _kh(o["sum_w"], n_ins, T)
+    assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
+    assert abs(r["sum_w"] - o["sum_w"]) <= KH_RTOL * o["sum_w"]
+    if o["sum_w"] > 0:
+        mean_o = o["sum_ew"] / o["sum_w"]
+        assert abs(r["mean_energy"] - mean_o) <= 1e-5 * abs(mean_o) + 1e-3
+    assert r["n_insertions"] == n_ins and r["n_blocked"] == 0
+
+
+def test_henry_config1_points(ctx):
+    """config-1 framework, 1e5 insertions at 298 K (CH4)."""
+    f = synth.config1(0)
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    r = ctx.henry(fw, 298.0, 100000, seed=1234)
+    o = oracle.henry(P, f.t_matrix, f.rep, f.rc2, 298.0, 1234, 100000)
+    kh_o = _kh(o["sum_w"], 100000, 298.0)
+    assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
+
+
+def test_henry_deterministic(ctx):
+    f, P, fw = _fw(ctx, 4)
+    a = ctx.henry(fw, 300.0, 50000, seed=9, want_energies=True)
+    b = ctx.henry(fw, 300.0, 50000, seed=9, want_energies=True)
+    assert np.array_equal(a["energies"], b["energies"]) and a["sum_w"] == b["sum_w"]
+    c = ctx.henry(fw, 300.0, 50000, seed=10)
+    assert c["sum_w"] != a["sum_w"]
+
+
+def test_henry_with_block_mask(ctx):
+    f, P, fw = _fw(ctx, 5, n_atoms=300)
+    T = 298.0
+    dims = (24, 24, 24)
+    g = ctx.grid(fw, dims).astype(np.float64)
+    rng = np.random.default_rng(0)
+    mask = (rng.random(dims) < 0.02).astype(np.uint8)
+    n = 60000
+    r = ctx.henry(fw, T, n, seed=77, block_mask=mask, want_energies=True)
+    o = oracle.henry(P, f.t_matrix, f.rep, f.rc2, T, 77, n, mask=mask, want_energies=True)
+    assert r["n_blocked"] == o["n_blocked"] > 0
+    blocked = np.isinf(o["energies"])
+    assert np.array_equal(np.isinf(r["energies"]), blocked)
+    kh_o = _kh(o["sum_w"], n, T)
+    assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
+    del g
+
+
+def test_henry_all_blocked(ctx):
+    f, P, fw = _fw(ctx, 6, n_atoms=50)
+    mask = np.ones((4, 4, 4), dtype=np.uint8)
+    r = ctx.henry(fw, 298.0, 5000, seed=1, block_mask=mask)
+    assert r["n_blocked"] == 5000 and r["sum_w"] == 0.0 and r["kh_mol_m3_pa"] == 0.0
+
+
+def test_henry_lse_form_consistent(ctx):
+    f, P, fw = _fw(ctx, 7)
+    r = ctx.henry(fw, 150.0, 20000, seed=3)
+    assert np.isclose(r["sum_w"], r["sum_w_scaled"] * np.exp(r["log_scale"]), rtol=1e-14)
+    assert np.isclose(r["mean_energy"], r["sum_ew_scaled"] / r["sum_w_scaled"], rtol=1e-14)
+
+
+def test_henry_invalid(ctx):
+    import emptyroom_b200 as er
+    f, P, fw = _fw(ctx, 8, n_atoms=20)
+    with pytest.raises(er.ErError):
+        ctx.henry(fw, -1.0, 100, seed=0)
+    with pytest.raises(er.ErError):
+        ctx.henry(fw, 298.0, 0, seed=0)

@@ -1,0 +1,98 @@
+"""Pins the CPU oracle (oracle/er_oracle.c) to the reference's own code.
+
+Two anchors: the golden fixtures in tests/golden (outputs of the reference's
+src/computegridsheet.h, src/pocketblocking.cc, src/Framework.cc and
+src/Forcefield.cc, produced by tests/golden/make_golden.py), and, where
+oracle/_ref/libref.so is present, the reference code run live on fresh
+seeded inputs. CPU only.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+
+GRID_CASES = ["grid_cubic", "grid_triclinic", "grid_rep2"]
+POCKET_CASES = ["pockets_a", "pockets_b", "pockets_perc", "pockets_perc_dense", "pockets_sparse"]
+
+
+@pytest.mark.parametrize("name", GRID_CASES)
+def test_oracle_grid_matches_golden_bitwise(name):
+    g = golden(name)
+    e = oracle.grid(g["particles"], g["t_matrix"], g["rep"], float(g["rc2"]), g["dims"])
+    assert np.array_equal(e, g["grid"])
+
+
+@pytest.mark.parametrize("name", GRID_CASES)
+def test_oracle_accessibility_matches_golden(name):
+    g = golden(name)
+    a = oracle.accessibility(g["particles"], g["t_matrix"], g["dims"])
+    assert np.array_equal(a, g["accessibility"])
+
+
+@pytest.mark.parametrize("name", GRID_CASES)
+def test_oracle_points_equal_grid(name):
+    """The point form (used for Widom) evaluates the same sum as the grid form."""
+    g = golden(name)
+    nx, ny, nz = (int(x) for x in g["dims"])
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    pts = np.stack([ii / (nx - 1), jj / (ny - 1), kk / (nz - 1)], axis=-1).reshape(-1, 3)
+    e = oracle.points(g["particles"], g["t_matrix"], g["rep"], float(g["rc2"]), pts, 1e-12)
+    assert np.array_equal(e.reshape(nx, ny, nz), g["grid"])
+
+
+@pytest.mark.parametrize("name", POCKET_CASES)
+def test_oracle_pockets_match_golden_bitwise(name):
+    g = golden(name)
+    blocked, n, seg = oracle.block_pockets(g["grid"], float(g["T"]))
+    assert n == int(g["n_pockets"])
+    assert np.array_equal(blocked, g["blocked"])
+    # segment ids: -1 exactly where E >= 15 T, and numbered in scan order
+    assert np.array_equal(seg < 0, g["grid"] >= 15.0 * float(g["T"]))
+    first = {}
+    for idx, s in enumerate(seg.ravel()):
+        if s >= 0 and s not in first:
+            first[s] = idx
+    assert list(first) == sorted(first)
+
+
+def test_philox_known_answers():
+    """Random123 known-answer vectors of Philox4x32-10 (Salmon et al., SC'11)."""
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+           ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+           ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+            (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1))]
+    for ctr, key, want in kat:
+        assert [int(x) for x in oracle.philox4x32_10(ctr, key)] == list(want)
+
+
+def test_insertion_points_uniform():
+    pts = np.array([oracle.insertion_point(7, i) for i in range(4000)])
+    assert pts.min() >= 0.0 and pts.max() < 1.0
+    assert np.all(np.abs(pts.mean(axis=0) - 0.5) < 0.02)
+    assert len(np.unique(pts[:, 0])) == len(pts)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("seed", [101, 102])
+def test_oracle_grid_matches_reference_live(seed):
+    from emptyroom_b200 import synth
+    fw = synth.make_framework(seed, (11.0 + seed % 3, 12.5, 10.0), (82.0, 97.0, 104.0), 30,
+                              probe="Kr", rc=10.0)
+    P = fw.particles()
+    dims = (7, 6, 8)
+    assert np.array_equal(oracle.grid(P, fw.t_matrix, fw.rep, fw.rc2, dims),
+                          oracle.ref_grid(P, fw.t_matrix, fw.rep, fw.rc2, dims))
+    assert np.array_equal(oracle.accessibility(P, fw.t_matrix, dims),
+                          oracle.ref_accessibility(P, fw.t_matrix, dims))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("seed,p", [(201, 0.25), (202, 0.32), (203, 0.5)])
+def test_oracle_pockets_match_reference_live(seed, p):
+    rng = np.random.default_rng(seed)
+    T = 250.0
+    E = np.where(rng.random((13, 11, 12)) < p, -T, 20 * T)
+    b1, n1, _ = oracle.block_pockets(E, T)
+    b2, n2 = oracle.ref_block_pockets(E, T)
+    assert n1 == n2 and np.array_equal(b1, b2)
