@@ -35,6 +35,14 @@ class ErGridJob(ctypes.Structure):
                 ("out_device", c_void_p)]
 
 
+class ErSettings(ctypes.Structure):
+    _fields_ = [("forcefield", ctypes.c_char * 256), ("verbose", c_int),
+                ("grid_resolution", c_double), ("grid_output_format", ctypes.c_char * 16),
+                ("r_cutoff_squared", c_double), ("feynman_hibbs", c_int),
+                ("energy_threshold", c_double), ("temperature", c_double),
+                ("insertions_per_a3", c_int)]
+
+
 class ErHenryResult(ctypes.Structure):
     _fields_ = [("sum_w", c_double), ("sum_ew", c_double), ("log_scale", c_double),
                 ("sum_w_scaled", c_double), ("sum_ew_scaled", c_double),
@@ -73,6 +81,30 @@ SIGNATURES = {
     "er_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
     "er_insertion_point": (None, [c_uint64, c_uint64, _dp]),
     "er_synth_positions": (c_int, [c_uint64, _dp, c_int, c_double, _dp]),
+    "er_structure_load": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(c_void_p),
+                                  ctypes.c_char_p, c_size_t]),
+    "er_structure_free": (None, [c_void_p]),
+    "er_structure_info": (c_int, [c_void_p, _ip, _dp, _dp, _dp, _dp, _dp]),
+    "er_structure_frac": (c_int, [c_void_p, _dp]),
+    "er_structure_label": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_size_t]),
+    "er_forcefield_load": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(c_void_p),
+                                   ctypes.c_char_p, c_size_t]),
+    "er_forcefield_free": (None, [c_void_p]),
+    "er_forcefield_count": (c_int, [c_void_p]),
+    "er_forcefield_entry": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_size_t, _dp, _dp]),
+    "er_forcefield_find": (c_int, [c_void_p, ctypes.c_char_p, _dp, _dp]),
+    "er_mix_particles": (c_int, [c_void_p, c_void_p, c_double, c_double, c_void_p,
+                                 ctypes.c_char_p, c_size_t]),
+    "er_adsorbate_mw": (c_int, [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_char_p,
+                                c_size_t]),
+    "er_read_uc": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _ip,
+                           ctypes.c_char_p, c_size_t]),
+    "er_write_uc": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _ip]),
+    "er_read_settings": (c_int, [ctypes.c_char_p, c_int, c_void_p, ctypes.c_char_p, c_size_t]),
+    "er_write_grid_txt": (c_int, [ctypes.c_char_p, _fp, c_int, c_int, c_int, c_int]),
+    "er_write_grid_cube": (c_int, [ctypes.c_char_p, _fp, c_int, c_int, c_int, _dp, c_int]),
+    "er_read_grid_txt": (c_int, [ctypes.c_char_p, _dp, c_size_t, _ip, ctypes.c_char_p,
+                                 c_size_t]),
     "er_version": (ctypes.c_char_p, []),
     "er_probe_fp32_rate": (c_int, [c_void_p, c_double, _dp]),
 }

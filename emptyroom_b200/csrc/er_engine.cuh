@@ -301,10 +301,19 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
             }
         }
     }
-    // --- shell list: cutoff tested per pair, borderline pairs flagged
-    const int rc2bits = __float_as_int(cc.rc2f);
-    const unsigned bul = (unsigned)bul_i;
-    unsigned bflag = 0;
+    // --- shell list: cutoff tested per pair, borderline pairs flagged.
+    // dd = r^2 - fl32(rc^2) is exact wherever |dd| is near the window
+    // (Sterbenz), so |dd| <= win selects exactly the pairs within bul ulps.
+    const float rc2f = cc.rc2f;
+    float win;
+    {
+        int e;
+        frexpf(rc2f, &e);
+        win = ldexpf((float)bul_i, e - 24);
+    }
+    bool bf[kP];
+#pragma unroll
+    for (int p = 0; p < kP; ++p) bf[p] = false;
     q = 0;
     while (q < n_sh) {
         const int qe = (PREC == PREC_COMP) ? min(q + kAccChunk, n_sh) : n_sh;
@@ -317,14 +326,14 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
             for (int p = 0; p < kP; ++p) {
                 float r2, u3, t;
                 pair_r2(px[p], py[p], pz[p], a, r2);
-                const int d = __float_as_int(r2) - rc2bits;
+                const float dd = __fsub_rn(r2, rc2f);
                 if (PREC == PREC_COUNT) {
-                    if (d < 0) acc[p] += 1.0f;
+                    if (dd < 0.f) acc[p] += 1.0f;
                 } else {
                     pair_ut(r2, a.w, nc6, u3, t);
-                    if (d < 0) acc[p] = __fmaf_rn(u3, t, acc[p]);
+                    if (dd < 0.f) acc[p] = __fmaf_rn(u3, t, acc[p]);
                 }
-                bflag |= ((unsigned)(d + (int)bul) <= 2u * bul) ? (1u << p) : 0u;
+                bf[p] = bf[p] || (fabsf(dd) <= win);
             }
         }
         if (PREC == PREC_COMP) {
@@ -340,6 +349,9 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         for (int p = 0; p < kP; ++p) hi[p] = __fadd_rn(hi[p], acc[p]);
     }
     // --- exact re-decision of borderline shell pairs (rare)
+    unsigned bflag = 0;
+#pragma unroll
+    for (int p = 0; p < kP; ++p) bflag |= bf[p] ? (1u << p) : 0u;
     bflag &= vmask;
     if (__any_sync(0xffffffffu, bflag != 0)) {
         for (int p = 0; p < kP; ++p) {
@@ -352,10 +364,10 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
                 const float4 a = s.cpos[c];
                 float r2;
                 pair_r2(px[p], py[p], pz[p], a, r2);
-                const int d = __float_as_int(r2) - rc2bits;
-                if ((unsigned)(d + (int)bul) <= 2u * bul) {
+                const float dd = __fsub_rn(r2, rc2f);
+                if (fabsf(dd) <= win) {
                     const bool ex = exact_in_cutoff(fw, f, s.cgid[c], cc.r2min);
-                    if (ex != (d < 0)) {
+                    if (ex != (dd < 0.f)) {
                         float e = 1.0f;
                         if (PREC != PREC_COUNT) {
                             float u3, t;

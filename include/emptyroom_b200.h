@@ -200,6 +200,95 @@ void er_insertion_point(uint64_t seed, uint64_t i, double out[3]);
 int er_synth_positions(uint64_t seed, const double t_matrix[9], int n_atoms, double d_min,
                        double* frac_out);
 
+/* ------------------------------------------------------------------ file formats */
+/* The reference's input files, read the way its loaders read them. Paths are
+ * relative to `root` (the reference runs from its project root). Errors are
+ * returned (ER_ERR_IO / ER_ERR_NOT_FOUND / ER_ERR_INVALID) with a message in
+ * err[0..errlen), never exit(). */
+
+/* A parsed .cssr structure: Framework(name) of src/Framework.cc:13-178 --
+ * <root>/data/structures/<name>.cssr (a b c; alpha beta gamma in degrees;
+ * atom count; a skipped title line; atom lines `idx label x_f y_f z_f ...`
+ * with coordinates wrapped by fmod(x, 1.0)) and masses from
+ * <root>/data/masses.def. */
+typedef struct er_structure er_structure;
+int er_structure_load(const char* root, const char* name, er_structure** out, char* err,
+                      size_t errlen);
+void er_structure_free(er_structure* s);
+/* cell[6] = a, b, c (A), alpha, beta, gamma (radians, as Framework stores them);
+ * t and inv row-major; volume (A^3); density (kg/m^3). */
+int er_structure_info(const er_structure* s, int* n_atoms, double cell[6], double t[9],
+                      double inv[9], double* volume, double* density);
+/* frac: n_atoms x 3 (after fmod). */
+int er_structure_frac(const er_structure* s, double* frac);
+/* Label of atom i into buf (NUL-terminated). */
+int er_structure_label(const er_structure* s, int i, char* buf, size_t len);
+
+/* A force field: Forcefield(name) of src/Forcefield.cc:15-54 --
+ * <root>/data/forcefields/<name>.def, first line skipped, lines `label eps sigma`. */
+typedef struct er_forcefield er_forcefield;
+int er_forcefield_load(const char* root, const char* name, er_forcefield** out, char* err,
+                       size_t errlen);
+void er_forcefield_free(er_forcefield* f);
+int er_forcefield_count(const er_forcefield* f);
+int er_forcefield_entry(const er_forcefield* f, int i, char* label, size_t len, double* eps,
+                        double* sig);
+/* First entry with this label (GrabGuestForceFieldParams, src/readsettings.h:276-294). */
+int er_forcefield_find(const er_forcefield* f, const char* label, double* eps, double* sig);
+
+/* FrameworkParticle array with Lorentz-Berthelot mixing against the guest:
+ * LoadFastFrameworkParticleArray, src/load_fast_particle_f_array.h:13-40.
+ * out holds n_atoms entries. ER_ERR_NOT_FOUND names the first missing label. */
+int er_mix_particles(const er_structure* s, const er_forcefield* f, double eps_guest,
+                     double sig_guest, er_particle* out, char* err, size_t errlen);
+
+/* Adsorbate molecular weight from <root>/data/masses.def (GetAdsorbateMW,
+ * src/readsettings.h:19-49). */
+int er_adsorbate_mw(const char* root, const char* adsorbate, double* mw, char* err,
+                    size_t errlen);
+
+/* Replication factors from <root>/data/uc_replications/<name>_<which>.uc
+ * (ReadUnitCellReplicationFile, src/readsettings.h:243-274). */
+int er_read_uc(const char* root, const char* name, const char* which, int rep[3], char* err,
+               size_t errlen);
+/* Writes the .uc file with er_replication_factors(t, rc, factor). */
+int er_write_uc(const char* root, const char* name, const char* which, const int rep[3]);
+
+/* simulation.input keys (src/readsettings.h:51-156): token scan, unknown words
+ * ignored, defaults as the reference's. */
+typedef struct {
+    char forcefield[256];       /* "None" when absent */
+    int verbose;
+    double grid_resolution;     /* -1 when absent */
+    char grid_output_format[16];/* "txt" default */
+    double r_cutoff_squared;    /* 12.5^2 default */
+    int feynman_hibbs;
+    double energy_threshold;
+    double temperature;         /* -1 when absent */
+    int insertions_per_a3;      /* -1 when absent */
+} er_settings;
+#define ER_SETTINGS_GRID 1
+#define ER_SETTINGS_HENRY 2
+/* Reads <path> and checks the keys the given tool requires (same checks and
+ * messages as the reference). */
+int er_read_settings(const char* path, int kind, er_settings* out, char* err, size_t errlen);
+
+/* Grid text file of src/writegrid.cu:142-147,260-269: header
+ * "%d %d %d  = (N_x,N_y,N_z) grid points (grid is in fractional coords). Endpoints included.\n"
+ * then one line per (x, y) pencil of N_z values "% 13.6E ". Values are printed
+ * from double(grid[k + j nz + i ny nz]). Formatting is split over n_threads
+ * host threads (0 = all cores); bytes are identical to a serial fprintf. */
+int er_write_grid_txt(const char* path, const float* grid, int nx, int ny, int nz,
+                      int n_threads);
+/* .cube variant of src/writegrid.cu:149-166,244-258: header from t, values in
+ * kJ/mol (x 8.314 / 1000), six per line, newline after each pencil. */
+int er_write_grid_cube(const char* path, const float* grid, int nx, int ny, int nz,
+                       const double t[9], int n_threads);
+/* Reader with the layout contract of src/gcmc.cc:293-345: fills out (capacity
+ * `cap` doubles, index k + j nz + i ny nz) and dims. */
+int er_read_grid_txt(const char* path, double* out, size_t cap, int dims[3], char* err,
+                     size_t errlen);
+
 /* ------------------------------------------------------------------ diagnostics */
 /* Measures the device's FP32 FMA issue rate with a chain of independent FFMAs
  * (FP32-pipe lane-instructions per second, whole GPU) over about `seconds`.
