@@ -72,6 +72,8 @@ SIGNATURES = {
     "er_batch_plan_destroy": (None, [c_void_p]),
     "er_henry": (c_int, [c_void_p, c_int, c_double, c_int64, c_uint64, _u8p, c_int, c_int,
                          c_int, ctypes.POINTER(ErHenryResult), _fp]),
+    "er_henry_stats_noalloc": (c_int, [c_void_p, c_void_p, c_int64, c_double,
+                                       ctypes.POINTER(ErHenryResult)]),
     "er_block_pockets": (c_int, [c_void_p, _dp, c_int, c_int, c_int, c_double, _ip, _ip]),
     "er_block_pockets_device": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_double,
                                         c_void_p, _ip]),

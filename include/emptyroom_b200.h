@@ -158,6 +158,23 @@ int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t
              const uint8_t* block_mask, int mnx, int mny, int mnz, er_henry_result* out,
              float* energies_out);
 
+/* Widom statistics of energies the caller already holds on the device,
+ * computed without allocating anything: no counterpart in the reference.
+ * For callers that cannot call cudaMalloc -- a code that reserves all of its
+ * device memory up front in its own pool, or a loop that cannot take the
+ * implicit synchronisation and unbounded latency of cudaMalloc/cudaFree.
+ * energies: device float[n] (an entry of +inf has weight 0 and is counted in
+ * n_blocked); result as er_henry's reduction (FP64 log-sum-exp, same block
+ * partition) with n_insertions = n. Its scratch is one file-scope static
+ * device array of 4097 x 32 bytes, held by every GPU that loads this library
+ * until the process exits; the first call on a device looks up that array's
+ * address, so make it before any stream capture. Calls that overlap on one
+ * GPU share the array and race. n above ER_HENRY_STATS_NOALLOC_MAX_N is
+ * rejected with ER_ERR_LIMIT. */
+#define ER_HENRY_STATS_NOALLOC_MAX_N 2147483647LL
+int er_henry_stats_noalloc(er_ctx* ctx, const float* energies, int64_t n, double temperature,
+                           er_henry_result* out);
+
 /* ------------------------------------------------------------------ pocket blocking */
 /* FindAndBlockPockets (src/pocketblocking.cc:126-391) on the GPU: points with
  * E >= 15 T are inaccessible; accessible points form 6-connected segments

@@ -1,0 +1,60 @@
+"""er_henry_stats_noalloc, the entry point for callers that cannot allocate
+device memory (a code that owns all of its device memory through its own
+pool, or a loop that cannot take cudaMalloc's implicit synchronisation).
+It reduces energies the caller holds on the device using only a static
+device array, and must give er_henry's statistics for the same energies.
+This file is collected last; each test builds its own inputs."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from emptyroom_b200 import _capi, synth
+from emptyroom_b200._capi import ErHenryResult
+
+pytestmark = pytest.mark.gpu
+
+KH_RTOL = 1e-6  # the K_H tolerance of the Widom parity tests
+
+
+def _noalloc(ctx, energies_dev, n, T):
+    out = ErHenryResult()
+    st = _capi.lib().er_henry_stats_noalloc(ctx.handle, ctypes.c_void_p(energies_dev), int(n),
+                                            float(T), ctypes.byref(out))
+    return st, out
+
+
+def _close(a, b):
+    return abs(a - b) <= KH_RTOL * abs(b)
+
+
+def test_noalloc_stats_match_er_henry_on_two_calls(ctx):
+    import torch
+    f = synth.make_framework(41, (25.8, 25.8, 25.8), (90, 90, 90), 300, probe="Xe")
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    T = 298.0
+    rng = np.random.default_rng(3)
+    mask = (rng.random((20, 20, 20)) < 0.03).astype(np.uint8)
+    runs = [ctx.henry(fw, T, 200000, seed=5, block_mask=mask, want_energies=True),
+            ctx.henry(fw, T, 70001, seed=6, want_energies=True)]
+    for ref in runs:  # two calls in a row, different sizes, the static array reused
+        E = torch.from_numpy(ref["energies"]).cuda()
+        st, got = _noalloc(ctx, E.data_ptr(), E.numel(), T)
+        assert st == 0, _capi.lib().er_ctx_last_error(ctx.handle)
+        assert _close(got.kh_mol_m3_pa, ref["kh_mol_m3_pa"])
+        assert _close(got.sum_w, ref["sum_w"])
+        assert _close(got.mean_energy, ref["mean_energy"])
+        assert got.n_insertions == ref["n_insertions"]
+        assert got.n_blocked == ref["n_blocked"]
+    assert runs[0]["n_blocked"] > 0
+    fw.release()
+
+
+def test_noalloc_rejects_out_of_range_sizes(ctx):
+    import torch
+    E = torch.zeros(16, dtype=torch.float32, device="cuda")
+    st, _ = _noalloc(ctx, E.data_ptr(), 0, 298.0)
+    assert st == 7  # ER_ERR_LIMIT
+    st, _ = _noalloc(ctx, E.data_ptr(), (1 << 31), 298.0)
+    assert st == 7
+    assert b"ER_HENRY_STATS_NOALLOC_MAX_N" in _capi.lib().er_ctx_last_error(ctx.handle)
