@@ -25,9 +25,12 @@ ER_PREC_COMP = 0x0
 ER_PREC_FP32 = 0x10
 ER_PREC_FP64 = 0x20
 ER_COUNT_PAIRS = 0x40
+ER_TILE_P8 = 0x80
+ER_PREC_NEAR64 = 0x08
 ER_BATCH_PERSISTENT = 0
 ER_BATCH_PLAIN = 1
 ER_BATCH_HOST_OUT = 0x100
+ER_BATCH_AUTOTUNE = 0x200
 ER_ENERGY_CAP = 1.0e30
 R_GAS = 8.314  # J/(mol K), src/henry.cu:169
 
@@ -277,6 +280,16 @@ class Context:
             out["energies"] = en
         return out
 
+    def henry_device_mask(self, fw, temperature, n_ins, seed, mask_ptr, mask_dims):
+        """er_henry with a pocket mask that already lives on the device."""
+        mnx, mny, mnz = (int(x) for x in mask_dims)
+        res = ErHenryResult()
+        self._check(_capi.lib().er_henry(
+            self._h, fw.id, float(temperature), int(n_ins), int(seed),
+            ctypes.cast(ctypes.c_void_p(int(mask_ptr)), ctypes.POINTER(ctypes.c_uint8)),
+            mnx, mny, mnz, ctypes.byref(res), None))
+        return {k: getattr(res, k) for k, _ in ErHenryResult._fields_}
+
     def block_pockets(self, grid, temperature, want_segments=False):
         """FindAndBlockPockets on a host float64 grid; returns (grid copy, n_pockets[, seg])."""
         g = np.array(grid, dtype=np.float64, copy=True, order="C")
@@ -318,6 +331,12 @@ class BatchPlan:
     def launches(self):
         n = ctypes.c_int(0)
         self.ctx._check(_capi.lib().er_batch_plan_launches(self._h, ctypes.byref(n)))
+        return n.value
+
+    def tile(self, job):
+        """Points per thread (4 or 8) of the kernel variant used for job `job`."""
+        n = ctypes.c_int(0)
+        self.ctx._check(_capi.lib().er_batch_plan_tile(self._h, int(job), ctypes.byref(n)))
         return n.value
 
     def close(self):

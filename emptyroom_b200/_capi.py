@@ -50,6 +50,18 @@ class ErHenryResult(ctypes.Structure):
                 ("mean_energy", c_double), ("kh_mol_m3_pa", c_double)]
 
 
+class ErJob(ctypes.Structure):
+    _fields_ = [("kind", c_int), ("fw_key", c_uint64), ("desc", c_void_p), ("nx", c_int),
+                ("ny", c_int), ("nz", c_int), ("temperature", c_double),
+                ("n_insertions", c_int64), ("seed", c_uint64), ("grid_out_host", c_void_p)]
+
+
+class ErJobStatus(ctypes.Structure):
+    _fields_ = [("done", c_int), ("status", c_int), ("grid_cache_hit", c_int),
+                ("submit_s", c_double), ("start_s", c_double), ("finish_s", c_double),
+                ("henry", ErHenryResult)]
+
+
 # name -> (restype, argtypes); every entry point declared in include/emptyroom_b200.h
 SIGNATURES = {
     "er_status_string": (ctypes.c_char_p, [c_int]),
@@ -70,6 +82,7 @@ SIGNATURES = {
     "er_batch_plan_run": (c_int, [c_void_p]),
     "er_batch_plan_launches": (c_int, [c_void_p, _ip]),
     "er_batch_plan_destroy": (None, [c_void_p]),
+    "er_batch_plan_tile": (c_int, [c_void_p, c_int, _ip]),
     "er_henry": (c_int, [c_void_p, c_int, c_double, c_int64, c_uint64, _u8p, c_int, c_int,
                          c_int, ctypes.POINTER(ErHenryResult), _fp]),
     "er_henry_stats_noalloc": (c_int, [c_void_p, c_void_p, c_int64, c_double,
@@ -83,6 +96,14 @@ SIGNATURES = {
     "er_philox4x32_10": (None, [_u32p, _u32p, _u32p]),
     "er_insertion_point": (None, [c_uint64, c_uint64, _dp]),
     "er_synth_positions": (c_int, [c_uint64, _dp, c_int, c_double, _dp]),
+    "er_server_create": (c_int, [c_void_p, c_size_t, c_int, ctypes.POINTER(c_void_p)]),
+    "er_server_submit": (c_int, [c_void_p, ctypes.POINTER(ErJob), ctypes.POINTER(c_uint64)]),
+    "er_server_poll": (c_int, [c_void_p, c_uint64, ctypes.POINTER(ErJobStatus)]),
+    "er_server_wait": (c_int, [c_void_p, c_uint64, c_double, ctypes.POINTER(ErJobStatus)]),
+    "er_server_grid": (c_int, [c_void_p, c_uint64, ctypes.POINTER(c_void_p)]),
+    "er_server_now": (c_double, [c_void_p]),
+    "er_server_bytes": (c_int, [c_void_p, ctypes.POINTER(c_size_t)]),
+    "er_server_destroy": (None, [c_void_p]),
     "er_structure_load": (c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(c_void_p),
                                   ctypes.c_char_p, c_size_t]),
     "er_structure_free": (None, [c_void_p]),

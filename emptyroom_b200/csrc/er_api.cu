@@ -81,14 +81,16 @@ CutoffConsts make_cutoff_consts(double rc2, double /*box_diag*/, double r2min) {
 }
 
 // ------------------------------------------------------------------ kernels
-template <int PREC>
+template <int PREC, int P>
 __global__ void __launch_bounds__(kThreads, 2) grid_kernel(const __grid_constant__ GridTask task) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
-    GridPolicy pol(&task, blockIdx.x);
-    process_cta<GridPolicy, PREC>(s, pol, task.fw, task.cc);
+    GridPolicy<P> pol(&task, blockIdx.x);
+    process_cta<GridPolicy<P>, PREC>(s, pol, task.fw, task.cc);
 }
 
+// One CTA per SM slot pulls (task, brick) items from the queue until it is
+// empty; each task carries its own kernel variant (4 or 8 points per thread).
 template <int PREC>
 __global__ void __launch_bounds__(kThreads, 2)
     grid_persistent_kernel(const GridTask* __restrict__ tasks, const WorkItem* __restrict__ items,
@@ -103,8 +105,13 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (it >= n_items) break;
         const WorkItem wi = items[it];
         const GridTask* t = tasks + wi.task;
-        GridPolicy pol(t, wi.brick);
-        process_cta<GridPolicy, PREC>(s, pol, t->fw, t->cc);
+        if (t->tile_p == 8) {
+            GridPolicy<8> pol(t, wi.brick);
+            process_cta<GridPolicy<8>, PREC>(s, pol, t->fw, t->cc);
+        } else {
+            GridPolicy<4> pol(t, wi.brick);
+            process_cta<GridPolicy<4>, PREC>(s, pol, t->fw, t->cc);
+        }
     }
 }
 
@@ -115,23 +122,35 @@ __global__ void f32_to_f64_kernel(const float* __restrict__ in, double* __restri
         out[i] = (double)in[i];
 }
 
-static int configure_kernels(er_ctx* ctx) {
+template <int P>
+static int configure_variant(er_ctx* ctx) {
     const int smem = (int)sizeof(EngineSmem);
-    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_COMP>,
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_COMP, P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_FP32>,
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_FP32, P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_COUNT>,
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_COUNT, P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_COMP>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_FP32>,
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_NEAR64, P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return ER_OK;
 }
 
+static int configure_kernels(er_ctx* ctx) {
+    int st = configure_variant<4>(ctx);
+    if (st == ER_OK) st = configure_variant<8>(ctx);
+    const int smem = (int)sizeof(EngineSmem);
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_COMP>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_FP32>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    return st;
+}
+
 int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, float* out,
-                   GridTask& t) {
+                   GridTask& t, int tile_p) {
+    if (tile_p != 4 && tile_p != 8)
+        return set_error(ctx, ER_ERR_INVALID, "grid: kernel variant must have P = 4 or 8");
     if (nx < 2 || ny < 2 || nz < 2)
         return set_error(ctx, ER_ERR_INVALID, "grid: nx, ny, nz must be >= 2 (axes i/(N-1))");
     if ((double)nx * ny * nz > 4.0e9)
@@ -139,27 +158,38 @@ int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, floa
     t.fw = fw.dev;
     t.cc = make_cutoff_consts(fw.rc2, 0.0, 1e-12 * 1e-12);  // min_r, src/computegridsheet.h:19
     t.nx = nx; t.ny = ny; t.nz = nz;
-    t.nb[0] = (nx + kBI - 1) / kBI;
-    t.nb[1] = (ny + kBJ - 1) / kBJ;
-    t.nb[2] = (nz + kBK - 1) / kBK;
+    t.tile_p = tile_p;
+    t.nb[0] = (nx + 2 * tile_p - 1) / (2 * tile_p);
+    t.nb[1] = (ny + 2 * kWJ - 1) / (2 * kWJ);
+    t.nb[2] = (nz + 2 * kWK - 1) / (2 * kWK);
     t.out = out;
     return ER_OK;
 }
 
 static int64_t task_bricks(const GridTask& t) { return (int64_t)t.nb[0] * t.nb[1] * t.nb[2]; }
 
-int launch_grid_plain(er_ctx* ctx, const GridTask& t, int prec) {
+int launch_grid_plain_on(er_ctx* ctx, const GridTask& t, int prec, cudaStream_t st) {
     const int64_t nbr = task_bricks(t);
     if (nbr > INT32_MAX) return set_error(ctx, ER_ERR_LIMIT, "grid: too many bricks");
     const size_t smem = sizeof(EngineSmem);
-    if (prec == PREC_FP32)
-        grid_kernel<PREC_FP32><<<(unsigned)nbr, kThreads, smem, ctx->stream>>>(t);
-    else if (prec == PREC_COUNT)
-        grid_kernel<PREC_COUNT><<<(unsigned)nbr, kThreads, smem, ctx->stream>>>(t);
-    else
-        grid_kernel<PREC_COMP><<<(unsigned)nbr, kThreads, smem, ctx->stream>>>(t);
+    const unsigned g = (unsigned)nbr;
+    if (t.tile_p == 8) {
+        if (prec == PREC_FP32) grid_kernel<PREC_FP32, 8><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_COUNT) grid_kernel<PREC_COUNT, 8><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_NEAR64) grid_kernel<PREC_NEAR64, 8><<<g, kThreads, smem, st>>>(t);
+        else grid_kernel<PREC_COMP, 8><<<g, kThreads, smem, st>>>(t);
+    } else {
+        if (prec == PREC_FP32) grid_kernel<PREC_FP32, 4><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_COUNT) grid_kernel<PREC_COUNT, 4><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_NEAR64) grid_kernel<PREC_NEAR64, 4><<<g, kThreads, smem, st>>>(t);
+        else grid_kernel<PREC_COMP, 4><<<g, kThreads, smem, st>>>(t);
+    }
     ER_CUDA(ctx, cudaGetLastError());
     return ER_OK;
+}
+
+int launch_grid_plain(er_ctx* ctx, const GridTask& t, int prec) {
+    return launch_grid_plain_on(ctx, t, prec, ctx->stream);
 }
 
 int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const WorkItem* d_items,
@@ -171,13 +201,65 @@ int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const WorkItem*
     per_sm = std::max(per_sm, 1);
     const int grid = std::min<int64_t>((int64_t)ctx->num_sms * per_sm, std::max(n_items, 1));
     ER_CUDA(ctx, cudaMemsetAsync(d_head, 0, sizeof(int), ctx->stream));
+    cudaStream_t st = ctx->stream;
     if (prec == PREC_FP32)
-        grid_persistent_kernel<PREC_FP32><<<grid, kThreads, smem, ctx->stream>>>(d_tasks, d_items,
-                                                                                 n_items, d_head);
+        grid_persistent_kernel<PREC_FP32><<<grid, kThreads, smem, st>>>(d_tasks, d_items, n_items,
+                                                                        d_head);
     else
-        grid_persistent_kernel<PREC_COMP><<<grid, kThreads, smem, ctx->stream>>>(d_tasks, d_items,
-                                                                                 n_items, d_head);
+        grid_persistent_kernel<PREC_COMP><<<grid, kThreads, smem, st>>>(d_tasks, d_items, n_items,
+                                                                        d_head);
     ER_CUDA(ctx, cudaGetLastError());
+    return ER_OK;
+}
+
+// ------------------------------------------------------------------ autotuner
+// Picks the kernel variant (4 or 8 points per thread) for a class of jobs by
+// timing both on the same sample of the job -- its first 16 x-layers, which
+// are whole bricks for both variants -- and caches the faster one per class:
+// (atoms per A^3 in half-octaves, smallest grid spacing in quarter-octaves,
+// cutoff in quarter-Angstroms).
+int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out, int* tile_p) {
+    const double rho = (double)std::max(f.n_atoms, 1) / std::max(f.volume, 1e-9);
+    double h = 1e30;
+    const int dims[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; ++d) h = std::min(h, f.cell_len[d] / std::max(dims[d] - 1, 1));
+    const std::tuple<int, int, int> key((int)lround(2.0 * log2(rho)), (int)lround(4.0 * log2(h)),
+                                        (int)lround(4.0 * sqrt(f.rc2)));
+    auto it = ctx->tune.find(key);
+    if (it != ctx->tune.end()) {
+        *tile_p = it->second;
+        return ER_OK;
+    }
+    cudaEvent_t e0, e1;
+    ER_CUDA(ctx, cudaEventCreate(&e0));
+    ER_CUDA(ctx, cudaEventCreate(&e1));
+    float best_ms = 0.f;
+    int best = 4;
+    for (int P : {4, 8}) {
+        GridTask t;
+        int st = fill_grid_task(ctx, f, nx, ny, nz, out, t, P);
+        if (st != ER_OK) return st;
+        if (nx >= 17) t.nb[0] = 16 / (2 * P);  // the first 16 x-layers only
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            ER_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+            st = launch_grid_plain(ctx, t, PREC_COMP);
+            if (st != ER_OK) return st;
+            ER_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+            ER_CUDA(ctx, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            ER_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) ms_min = std::min(ms_min, ms);  // rep 0 warms up
+        }
+        if (P == 4 || ms_min < best_ms) {
+            best_ms = ms_min;
+            best = P;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->tune[key] = best;
+    *tile_p = best;
     return ER_OK;
 }
 
@@ -224,12 +306,11 @@ void er_ctx_destroy(er_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->fws) cudaFree(kv.second.block);
     ctx->fws.clear();
-    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->tasks,   &ctx->items,  &ctx->counter, &ctx->h_pts,
-                      &ctx->h_bin,    &ctx->h_order, &ctx->h_tmp,  &ctx->h_counts, &ctx->h_starts,
-                      &ctx->h_wt,     &ctx->h_nwt,   &ctx->h_e,    &ctx->h_part,  &ctx->h_mask,
-                      &ctx->h_res,    &ctx->p_grid,  &ctx->p_lab,  &ctx->p_seg,   &ctx->p_flags,
-                      &ctx->p_misc,   &ctx->p_mask,  &ctx->sheet_cache.grid};
+    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->tasks,  &ctx->items,  &ctx->counter,
+                      &ctx->p_grid,   &ctx->p_lab,  &ctx->p_seg,  &ctx->p_flags,
+                      &ctx->p_misc,   &ctx->p_mask, &ctx->sheet_cache.grid};
     for (DevBuf* b : bufs) b->release();
+    ctx->henry.release();
     ctx->pinned.release();
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -263,43 +344,41 @@ int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) 
     const size_t s_id = al(std::max<size_t>(n_img, 1) * sizeof(uint32_t));
     const size_t s_cs = al(hf.cell_start.size() * sizeof(int));
     const size_t s_af = al(std::max<size_t>(hf.atom_frac.size(), 1) * sizeof(HostImage));
-    const size_t total = s_xyz + s_par + s_id + s_cs + s_af;
+    const size_t s_lj = al(std::max<size_t>(hf.atom_lj64.size(), 2) * sizeof(double));
+    const size_t total = s_xyz + s_par + s_id + s_cs + s_af + s_lj;
     FwRecord rec;
     if (cudaMalloc(&rec.block, total) != cudaSuccess) {
         cudaGetLastError();
         return set_error(ctx, ER_ERR_NOMEM, "framework upload: device allocation failed");
     }
-    char* b = (char*)rec.block;
-    char* p_xyz = b;
-    char* p_par = p_xyz + s_xyz;
-    char* p_id = p_par + s_par;
-    char* p_cs = p_id + s_id;
-    char* p_af = p_cs + s_cs;
-    cudaError_t e = cudaSuccess;
-    if (n_img) {
-        if (e == cudaSuccess) e = cudaMemcpy(p_xyz, hf.img_xyz.data(), n_img * sizeof(HostImage),
-                                             cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(p_par, hf.img_par.data(),
-                                             n_img * 2 * sizeof(float), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(p_id, hf.img_id.data(), n_img * sizeof(uint32_t),
-                                             cudaMemcpyHostToDevice);
+    // one pinned host image of the whole block, one copy
+    if (ctx->pinned.ensure(total) != ER_OK) {
+        cudaFree(rec.block);
+        return set_error(ctx, ER_ERR_NOMEM, "framework upload: pinned staging failed");
     }
-    if (e == cudaSuccess) e = cudaMemcpy(p_cs, hf.cell_start.data(),
-                                         hf.cell_start.size() * sizeof(int),
-                                         cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !hf.atom_frac.empty())
-        e = cudaMemcpy(p_af, hf.atom_frac.data(), hf.atom_frac.size() * sizeof(HostImage),
-                       cudaMemcpyHostToDevice);
+    const size_t o_par = s_xyz, o_id = o_par + s_par, o_cs = o_id + s_id, o_af = o_cs + s_cs,
+                 o_lj = o_af + s_af;
+    char* h = (char*)ctx->pinned.ptr;
+    memcpy(h, hf.img_xyz.data(), n_img * sizeof(HostImage));
+    memcpy(h + o_par, hf.img_par.data(), n_img * 2 * sizeof(float));
+    memcpy(h + o_id, hf.img_id.data(), n_img * sizeof(uint32_t));
+    memcpy(h + o_cs, hf.cell_start.data(), hf.cell_start.size() * sizeof(int));
+    memcpy(h + o_af, hf.atom_frac.data(), hf.atom_frac.size() * sizeof(HostImage));
+    memcpy(h + o_lj, hf.atom_lj64.data(), hf.atom_lj64.size() * sizeof(double));
+    cudaError_t e = cudaMemcpyAsync(rec.block, h, total, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         cudaFree(rec.block);
         return cuda_error(ctx, e, "framework upload: copy");
     }
+    char* b = (char*)rec.block;
     FwDev& d = rec.dev;
-    d.img_xyz = (const double4*)p_xyz;
-    d.img_par = (const float2*)p_par;
-    d.img_id = (const uint32_t*)p_id;
-    d.cell_start = (const int*)p_cs;
-    d.atom_frac = (const double4*)p_af;
+    d.img_xyz = (const double4*)b;
+    d.img_par = (const float2*)(b + o_par);
+    d.img_id = (const uint32_t*)(b + o_id);
+    d.cell_start = (const int*)(b + o_cs);
+    d.atom_frac = (const double4*)(b + o_af);
+    d.atom_lj64 = (const double2*)(b + o_lj);
     d.n_img = (int)n_img;
     d.n_atoms = hf.n_atoms;
     for (int k = 0; k < 3; ++k) {
@@ -352,9 +431,11 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const FwRecord* f = find_fw(ctx, fw_id);
     if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "grid: unknown framework id");
-    const int prec = (flags & ER_COUNT_PAIRS) ? PREC_COUNT
-                     : (flags & ER_PREC_FP32) ? PREC_FP32
-                                              : PREC_COMP;
+    const int tile_p = (flags & ER_TILE_P8) ? 8 : 4;
+    const int prec = (flags & ER_COUNT_PAIRS)   ? PREC_COUNT
+                     : (flags & ER_PREC_FP32)   ? PREC_FP32
+                     : (flags & ER_PREC_NEAR64) ? PREC_NEAR64
+                                                : PREC_COMP;
     if (flags & ER_PREC_FP64)
         return set_error(ctx, ER_ERR_INVALID, "grid: ER_PREC_FP64 is served by er_grid_fp64");
     const size_t npts = (size_t)nx * ny * nz;
@@ -369,7 +450,7 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
         dst = (float*)ctx->grid_f32.ptr;
     }
     GridTask t;
-    int st = fill_grid_task(ctx, *f, nx, ny, nz, dst, t);
+    int st = fill_grid_task(ctx, *f, nx, ny, nz, dst, t, tile_p);
     if (st != ER_OK) return st;
     st = launch_grid_plain(ctx, t, prec);
     if (st != ER_OK) return st;
@@ -472,6 +553,8 @@ extern "C" {
 int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode,
                          er_batch_plan** out) {
     if (!ctx || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return ER_ERR_INVALID;
+    const bool autotune = (mode & ER_BATCH_AUTOTUNE) != 0;
+    mode &= ~ER_BATCH_AUTOTUNE;
     if (mode != ER_BATCH_PERSISTENT && mode != ER_BATCH_PLAIN) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     *out = nullptr;
@@ -487,8 +570,15 @@ int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int m
             return set_error(ctx, f ? ER_ERR_INVALID : ER_ERR_NOT_FOUND,
                              "batch: unknown framework id or NULL output");
         }
+        int tile_p = 4;
+        int st = ER_OK;
+        if (autotune && jobs[i].nx >= 2 && jobs[i].ny >= 2 && jobs[i].nz >= 2)
+            st = tune_tile(ctx, *f, jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].out_device,
+                           &tile_p);
         GridTask t;
-        int st = fill_grid_task(ctx, *f, jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].out_device, t);
+        if (st == ER_OK)
+            st = fill_grid_task(ctx, *f, jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].out_device, t,
+                                tile_p);
         if (st != ER_OK) {
             delete p;
             return st;
@@ -560,6 +650,12 @@ int er_batch_plan_run(er_batch_plan* p) {
 int er_batch_plan_launches(const er_batch_plan* p, int* n) {
     if (!p || !n) return ER_ERR_INVALID;
     *n = p->launches;
+    return ER_OK;
+}
+
+int er_batch_plan_tile(const er_batch_plan* p, int job, int* tile_p) {
+    if (!p || !tile_p || job < 0 || job >= p->n_jobs) return ER_ERR_INVALID;
+    *tile_p = p->tasks[job].tile_p;
     return ER_OK;
 }
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -40,6 +41,26 @@ struct HostBuf {
     void release();
 };
 
+// Device scratch of one Widom pipeline (er_henry.cu); one per stream that
+// runs Widom jobs concurrently.
+struct HenryScratch {
+    DevBuf pts, bin, order, tmp, counts, starts, e, nblk, part, res, mask;
+    size_t bytes() const {
+        return pts.cap + bin.cap + order.cap + tmp.cap + counts.cap + starts.cap + e.cap +
+               nblk.cap + part.cap + res.cap + mask.cap;
+    }
+    void release() {
+        DevBuf* b[] = {&pts, &bin, &order, &tmp, &counts, &starts, &e, &nblk, &part, &res, &mask};
+        for (DevBuf* x : b) x->release();
+    }
+};
+
+// Host copy of a Widom reduction: (m, s, se) and the blocked count.
+struct HenryOut {
+    double lse[3];
+    int n_blocked;
+};
+
 }  // namespace er
 
 struct er_ctx {
@@ -50,6 +71,7 @@ struct er_ctx {
     std::map<int, er::FwRecord> fws;
     int next_fw = 1;
     double cell_edge = 2.0;  // cell-list edge (A)
+    std::map<std::tuple<int, int, int>, int> tune;  // autotuned kernel variant per job class
     // scratch
     er::DevBuf grid_f32;     // staging for host-bound grids
     er::DevBuf tasks;        // GridTask arrays for batches
@@ -57,8 +79,7 @@ struct er_ctx {
     er::DevBuf counter;      // persistent-queue heads
     er::HostBuf pinned;      // pinned staging
     // Widom scratch
-    er::DevBuf h_pts, h_bin, h_order, h_tmp, h_counts, h_starts, h_wt, h_nwt, h_e, h_part,
-        h_mask, h_res;
+    er::HenryScratch henry;
     // pocket-blocking scratch
     er::DevBuf p_grid, p_lab, p_seg, p_flags, p_misc, p_mask;
     // device-resident grid cache for er_grid_sheet: key (fw, nx, ny, nz)
@@ -75,6 +96,18 @@ int cuda_error(er_ctx* ctx, cudaError_t e, const char* what);
 const FwRecord* find_fw(er_ctx* ctx, int fw_id);
 // Cutoff constants for a framework and a CTA box diagonal (A).
 CutoffConsts make_cutoff_consts(double rc2, double box_diag, double r2min);
+// Fills a grid task (validates dims) and launches the plain grid kernel on `st`.
+int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, float* out,
+                   GridTask& t, int tile_p = 4);
+int launch_grid_plain_on(er_ctx* ctx, const GridTask& t, int prec, cudaStream_t st);
+// Widom pipeline on stream `st` with scratch `hs`; when host_out (pinned) is
+// given, the reduction and the blocked count are copied there asynchronously.
+int henry_check(er_ctx* ctx, double temperature, int64_t n_ins, const uint8_t* block_mask,
+                int mnx, int mny, int mnz);
+int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, uint64_t seed,
+                  const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
+                  HenryScratch& hs, HenryOut* host_out);
+void henry_finish(const HenryOut& h, int64_t n, double temperature, er_henry_result* out);
 
 }  // namespace er
 

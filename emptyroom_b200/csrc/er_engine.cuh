@@ -35,9 +35,9 @@ namespace er {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr int kP = 4;                      // points per thread
+// points per thread (P) and the CTA brick are set by the point policy (Tile)
 constexpr int kWJ = 4, kWK = 8;            // lanes of a warp sub-brick along j, k
-constexpr int kBI = kP * 2, kBJ = kWJ * 2, kBK = kWK * 2;  // CTA brick 8 x 8 x 16 points
+constexpr int kPMax = 8;                   // largest P any policy uses
 constexpr int kMaxCand = 2048;             // CTA candidate capacity per flush
 constexpr int kRowChunk = kThreads;        // cell rows examined per producer pass
 constexpr int kAccChunk = 64;              // atoms per FP32 partial sum
@@ -45,13 +45,37 @@ constexpr float kEnergyCap = 1.0e30f;      // overflow cap (ER_ENERGY_CAP)
 
 // PREC_COUNT writes the number of in-cutoff pair terms per point instead of
 // the energy (same traversal; used to count the algorithmic work of a job).
-enum { PREC_COMP = 0, PREC_FP32 = 1, PREC_COUNT = 2 };
+// PREC_NEAR64 is PREC_COMP with the pairs of atoms within kNearR of a warp's
+// box evaluated in FP64 (they carry most of |E| where terms cancel).
+enum { PREC_COMP = 0, PREC_FP32 = 1, PREC_COUNT = 2, PREC_NEAR64 = 3 };
+
+template <int PREC>
+struct PrecTraits {
+    static constexpr bool comp = PREC == PREC_COMP || PREC == PREC_NEAR64;
+    static constexpr bool near64 = PREC == PREC_NEAR64;
+};
+
+constexpr int kNearCap = 256;     // near-list capacity per warp (overflow stays FP32)
+constexpr float kNearR = 5.0f;    // near radius (A) from the warp box
+
+// One candidate atom image in shared memory (32 bytes, so a list entry can be
+// the byte offset of its record and a load needs no index arithmetic).
+struct __align__(32) Cand {
+    float4 p;    // (dx, dy, dz, C12), position relative to the CTA centre
+    float nc6;   // -C6
+    int id;      // image index (for the FP64 re-decision)
+    float pad0, pad1;
+};
+
+__device__ __forceinline__ const Cand& cand_at(const Cand* base, unsigned off) {
+    return *reinterpret_cast<const Cand*>(reinterpret_cast<const char*>(base) + off);
+}
 
 struct __align__(16) EngineSmem {
-    float4 cpos[kMaxCand];                 // (dx, dy, dz, C12) relative to the CTA centre
-    float cnc6[kMaxCand];                  // -C6
-    int cgid[kMaxCand];                    // image index (for the FP64 re-decision)
-    unsigned short wl[kWarps][kMaxCand];   // per-warp inner (front) / shell (back) lists
+    Cand cand[kMaxCand];                   // CTA candidates
+    unsigned short wl[kWarps][kMaxCand];   // per-warp inner (front) / shell (back) lists of
+                                           // byte offsets into cand
+    unsigned short wn[kWarps][kNearCap];   // per-warp near lists (PREC_NEAR64)
     int row_beg[kRowChunk];
     int row_off[kRowChunk];
     int warp_tot[kWarps];
@@ -151,8 +175,13 @@ __device__ __forceinline__ void two_sum_into(float& hi, float& lo, float a) {
 // Point sources. A policy maps (warp, lane, p) to an FP64 fractional point
 // and stores its energy.
 
-// Lattice points of one 8 x 8 x 16 brick of a grid job.
+// Lattice points of one (2P) x 8 x 16 brick of a grid job: warp w owns the
+// P x 4 x 8 sub-brick at ((w & 1) P, ((w >> 1) & 1) 4, (w >> 2) 8); lane l the
+// (j, k) = (l / 8, l % 8) column of it and its P points along i.
+template <int P_>
 struct GridPolicy {
+    static constexpr int kP = P_;
+    static constexpr int kBI = 2 * P_, kBJ = 2 * kWJ, kBK = 2 * kWK;
     const GridTask* T;
     int i0, j0, k0;
     __device__ GridPolicy(const GridTask* task, int brick) : T(task) {
@@ -186,9 +215,11 @@ struct GridPolicy {
     }
 };
 
-// Widom insertion points: CTA c owns sorted positions [1024 c, 1024 c + 1024)
-// of `order`; warp w the 128 positions from 1024 c + 128 w.
+// Widom insertion points: CTA c owns sorted positions [256 P c, 256 P (c + 1))
+// of `order`; warp w the 32 P positions from 256 P c + 32 P w.
+template <int P_>
 struct PointPolicy {
+    static constexpr int kP = P_;
     const PointTask* T;
     int base, nv;
     __device__ PointPolicy(const PointTask* task, int cta)
@@ -235,20 +266,25 @@ template <class Pol, int PREC>
 __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
                                            const CutoffConsts& cc, int n_cand,
                                            const float* px, const float* py, const float* pz,
-                                           float* hi, float* lo, float wl0x, float wl0y,
-                                           float wl0z, float wh0x, float wh0y, float wh0z,
-                                           bool warp_live, unsigned vmask, int bul_i) {
+                                           float* hi, float* lo, double* nacc, float wl0x,
+                                           float wl0y, float wl0z, float wh0x, float wh0y,
+                                           float wh0z, bool warp_live, unsigned vmask,
+                                           int bul_i) {
+    constexpr bool kComp = PrecTraits<PREC>::comp;
+    constexpr bool kNear = PrecTraits<PREC>::near64;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (!warp_live) return;
     unsigned short* wl = s.wl[w];
-    // --- split candidates into inner / shell lists for this warp's box
-    int n_in = 0, n_sh = 0;
+    unsigned short* wn = s.wn[w];
+    // --- split candidates into inner / shell (/ near) lists for this warp's box
+    int n_in = 0, n_sh = 0, n_near = 0;
     const unsigned lt = (1u << lane) - 1u;
+    const float rnear2 = kNearR * kNearR;
     for (int base = 0; base < n_cand; base += 32) {
         const int c = base + lane;
-        bool in = false, sh = false;
+        bool in = false, sh = false, nr = false;
         if (c < n_cand) {
-            const float4 a = s.cpos[c];
+            const float4 a = s.cand[c].p;
             const float ex = fmaxf(0.f, fmaxf(wl0x - a.x, a.x - wh0x));
             const float ey = fmaxf(0.f, fmaxf(wl0y - a.y, a.y - wh0y));
             const float ez = fmaxf(0.f, fmaxf(wl0z - a.z, a.z - wh0z));
@@ -259,30 +295,42 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
             const float dmax2 = fx * fx + fy * fy + fz * fz;
             in = dmax2 < cc.rin2;
             sh = !in && dmin2 < cc.rout2;
+            nr = kNear && in && dmin2 < rnear2;
+        }
+        const unsigned short off = (unsigned short)(c * (int)sizeof(Cand));
+        if (kNear) {
+            const unsigned bn = __ballot_sync(0xffffffffu, nr);
+            const int at = n_near + __popc(bn & lt);
+            if (nr && at >= kNearCap) nr = false;  // overflow: stays on the FP32 inner list
+            if (nr) {
+                wn[at] = off;
+                in = false;
+            }
+            n_near = min(kNearCap, n_near + __popc(bn));
         }
         const unsigned bi = __ballot_sync(0xffffffffu, in);
         const unsigned bs = __ballot_sync(0xffffffffu, sh);
-        if (in) wl[n_in + __popc(bi & lt)] = (unsigned short)c;
-        if (sh) wl[kMaxCand - 1 - (n_sh + __popc(bs & lt))] = (unsigned short)c;
+        if (in) wl[n_in + __popc(bi & lt)] = off;
+        if (sh) wl[kMaxCand - 1 - (n_sh + __popc(bs & lt))] = off;
         n_in += __popc(bi);
         n_sh += __popc(bs);
     }
     __syncwarp();
 
     // --- inner list: every pair is inside the cutoff
-    float acc[kP];
+    float acc[Pol::kP];
 #pragma unroll
-    for (int p = 0; p < kP; ++p) acc[p] = 0.f;
+    for (int p = 0; p < Pol::kP; ++p) acc[p] = 0.f;
     int q = 0;
     while (q < n_in) {
-        const int qe = (PREC == PREC_COMP) ? min(q + kAccChunk, n_in) : n_in;
+        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
 #pragma unroll 2
         for (; q < qe; ++q) {
-            const int c = wl[q];
-            const float4 a = s.cpos[c];
-            const float nc6 = s.cnc6[c];
+            const Cand& cd = cand_at(s.cand, wl[q]);
+            const float4 a = cd.p;
+            const float nc6 = cd.nc6;
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
+            for (int p = 0; p < Pol::kP; ++p) {
                 if (PREC == PREC_COUNT) {
                     acc[p] += 1.0f;
                 } else {
@@ -293,9 +341,9 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
                 }
             }
         }
-        if (PREC == PREC_COMP) {
+        if (kComp) {
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
+            for (int p = 0; p < Pol::kP; ++p) {
                 two_sum_into(hi[p], lo[p], acc[p]);
                 acc[p] = 0.f;
             }
@@ -311,19 +359,19 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         frexpf(rc2f, &e);
         win = ldexpf((float)bul_i, e - 24);
     }
-    bool bf[kP];
+    bool bf[Pol::kP];
 #pragma unroll
-    for (int p = 0; p < kP; ++p) bf[p] = false;
+    for (int p = 0; p < Pol::kP; ++p) bf[p] = false;
     q = 0;
     while (q < n_sh) {
-        const int qe = (PREC == PREC_COMP) ? min(q + kAccChunk, n_sh) : n_sh;
+        const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
 #pragma unroll 2
         for (; q < qe; ++q) {
-            const int c = wl[kMaxCand - 1 - q];
-            const float4 a = s.cpos[c];
-            const float nc6 = s.cnc6[c];
+            const Cand& cd = cand_at(s.cand, wl[kMaxCand - 1 - q]);
+            const float4 a = cd.p;
+            const float nc6 = cd.nc6;
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
+            for (int p = 0; p < Pol::kP; ++p) {
                 float r2, u3, t;
                 pair_r2(px[p], py[p], pz[p], a, r2);
                 const float dd = __fsub_rn(r2, rc2f);
@@ -336,50 +384,83 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
                 bf[p] = bf[p] || (fabsf(dd) <= win);
             }
         }
-        if (PREC == PREC_COMP) {
+        if (kComp) {
 #pragma unroll
-            for (int p = 0; p < kP; ++p) {
+            for (int p = 0; p < Pol::kP; ++p) {
                 two_sum_into(hi[p], lo[p], acc[p]);
                 acc[p] = 0.f;
             }
         }
     }
-    if (PREC != PREC_COMP) {
+    if (!kComp) {
 #pragma unroll
-        for (int p = 0; p < kP; ++p) hi[p] = __fadd_rn(hi[p], acc[p]);
+        for (int p = 0; p < Pol::kP; ++p) hi[p] = __fadd_rn(hi[p], acc[p]);
     }
     // --- exact re-decision of borderline shell pairs (rare)
     unsigned bflag = 0;
 #pragma unroll
-    for (int p = 0; p < kP; ++p) bflag |= bf[p] ? (1u << p) : 0u;
+    for (int p = 0; p < Pol::kP; ++p) bflag |= bf[p] ? (1u << p) : 0u;
     bflag &= vmask;
     if (__any_sync(0xffffffffu, bflag != 0)) {
-        for (int p = 0; p < kP; ++p) {
+        for (int p = 0; p < Pol::kP; ++p) {
             if (!(bflag & (1u << p))) continue;
             double f[3];
             pol.point(w, lane, p, f);
             float corr = 0.f;
             for (int qq = 0; qq < n_sh; ++qq) {
-                const int c = wl[kMaxCand - 1 - qq];
-                const float4 a = s.cpos[c];
+                const Cand& cd = cand_at(s.cand, wl[kMaxCand - 1 - qq]);
+                const float4 a = cd.p;
                 float r2;
                 pair_r2(px[p], py[p], pz[p], a, r2);
                 const float dd = __fsub_rn(r2, rc2f);
                 if (fabsf(dd) <= win) {
-                    const bool ex = exact_in_cutoff(fw, f, s.cgid[c], cc.r2min);
+                    const bool ex = exact_in_cutoff(fw, f, cd.id, cc.r2min);
                     if (ex != (dd < 0.f)) {
                         float e = 1.0f;
                         if (PREC != PREC_COUNT) {
                             float u3, t;
-                            pair_ut(r2, a.w, s.cnc6[c], u3, t);
+                            pair_ut(r2, a.w, cd.nc6, u3, t);
                             e = __fmul_rn(u3, t);
                         }
                         corr = ex ? __fadd_rn(corr, e) : __fsub_rn(corr, e);
                     }
                 }
             }
-            if (PREC == PREC_COMP) two_sum_into(hi[p], lo[p], corr);
+            if (kComp) two_sum_into(hi[p], lo[p], corr);
             else hi[p] = __fadd_rn(hi[p], corr);
+        }
+    }
+    // --- near list in FP64: exact positions (FP64 images and points relative
+    // to the CTA centre) and FP64 (C12, C6); all near atoms are inner atoms.
+    if (kNear && n_near > 0) {
+        const double o0 = 0.5 * (s.box[0] + s.box[3]);
+        const double o1 = 0.5 * (s.box[1] + s.box[4]);
+        const double o2 = 0.5 * (s.box[2] + s.box[5]);
+        double qx[Pol::kP], qy[Pol::kP], qz[Pol::kP];
+#pragma unroll
+        for (int p = 0; p < Pol::kP; ++p) {
+            double f[3], x, y, z;
+            pol.point(w, lane, p, f);
+            frac_to_cart(fw.t, f[0], f[1], f[2], x, y, z);
+            qx[p] = x - o0;
+            qy[p] = y - o1;
+            qz[p] = z - o2;
+        }
+        for (int q = 0; q < n_near; ++q) {
+            const Cand& cd = cand_at(s.cand, wn[q]);
+            const double4 a = fw.img_xyz[cd.id];
+            const int atom = (int)(fw.img_id[cd.id] / (uint32_t)fw.imgs_per_atom);
+            const double2 lj = fw.atom_lj64[atom];
+            const double ax = a.x - o0, ay = a.y - o1, az = a.z - o2;
+#pragma unroll
+            for (int p = 0; p < Pol::kP; ++p) {
+                const double dx = qx[p] - ax, dy = qy[p] - ay, dz = qz[p] - az;
+                double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                r2 = fmax(r2, cc.r2min);
+                const double u = __drcp_rn(r2);
+                const double u3 = u * u * u;
+                nacc[p] = fma(u3, fma(lj.x, u3, -lj.y), nacc[p]);
+            }
         }
     }
 }
@@ -390,12 +471,12 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 
     // 1. FP64 Cartesian points and the CTA box.
-    double cx[kP], cy[kP], cz[kP];
+    double cx[Pol::kP], cy[Pol::kP], cz[Pol::kP];
     unsigned vmask = 0;
     double mn0 = INFINITY, mn1 = INFINITY, mn2 = INFINITY;
     double mx0 = -INFINITY, mx1 = -INFINITY, mx2 = -INFINITY;
 #pragma unroll
-    for (int p = 0; p < kP; ++p) {
+    for (int p = 0; p < Pol::kP; ++p) {
         double f[3];
         const bool ok = pol.point(w, lane, p, f);
         frac_to_cart(fw.t, f[0], f[1], f[2], cx[p], cy[p], cz[p]);
@@ -437,11 +518,14 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
         sqrt((hi0 - lo0) * (hi0 - lo0) + (hi1 - lo1) * (hi1 - lo1) + (hi2 - lo2) * (hi2 - lo2)));
 
     // 2. local FP32 coordinates and the warp box
-    float px[kP], py[kP], pz[kP], hi[kP], lo[kP];
+    float px[Pol::kP], py[Pol::kP], pz[Pol::kP], hi[Pol::kP], lo[Pol::kP];
+    double nacc[PrecTraits<PREC>::near64 ? Pol::kP : 1];
+#pragma unroll
+    for (int p = 0; p < (PrecTraits<PREC>::near64 ? Pol::kP : 1); ++p) nacc[p] = 0.0;
     float wl0x = INFINITY, wl0y = INFINITY, wl0z = INFINITY;
     float wh0x = -INFINITY, wh0y = -INFINITY, wh0z = -INFINITY;
 #pragma unroll
-    for (int p = 0; p < kP; ++p) {
+    for (int p = 0; p < Pol::kP; ++p) {
         px[p] = (float)(cx[p] - o0);
         py[p] = (float)(cy[p] - o1);
         pz[p] = (float)(cz[p] - o2);
@@ -535,15 +619,16 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                 const int pos = block_exscan(pass, s.warp_tot, &npass);
                 if (n_cand + npass > kMaxCand) {
                     __syncthreads();
-                    warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, wl0x, wl0y,
-                                          wl0z, wh0x, wh0y, wh0z, warp_live, vmask, bul);
+                    warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, nacc, wl0x,
+                                          wl0y, wl0z, wh0x, wh0y, wh0z, warp_live, vmask, bul);
                     __syncthreads();
                     n_cand = 0;
                 }
                 if (pass) {
-                    s.cpos[n_cand + pos] = cp;
-                    s.cnc6[n_cand + pos] = nc6;
-                    s.cgid[n_cand + pos] = g;
+                    Cand& dst = s.cand[n_cand + pos];
+                    dst.p = cp;
+                    dst.nc6 = nc6;
+                    dst.id = g;
                 }
                 n_cand += npass;
             }
@@ -552,14 +637,18 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     }
     if (n_cand > 0) {
         __syncthreads();
-        warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, wl0x, wl0y, wl0z,
-                              wh0x, wh0y, wh0z, warp_live, vmask, bul);
+        warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, nacc, wl0x, wl0y,
+                              wl0z, wh0x, wh0y, wh0z, warp_live, vmask, bul);
     }
     // 4. store
 #pragma unroll
-    for (int p = 0; p < kP; ++p) {
+    for (int p = 0; p < Pol::kP; ++p) {
         if (vmask & (1u << p)) {
-            float e = (PREC == PREC_COMP) ? __fadd_rn(hi[p], lo[p]) : hi[p];
+            float e;
+            if (PrecTraits<PREC>::near64)
+                e = (float)(((double)hi[p] + (double)lo[p]) + nacc[PrecTraits<PREC>::near64 ? p : 0]);
+            else
+                e = PrecTraits<PREC>::comp ? __fadd_rn(hi[p], lo[p]) : hi[p];
             if (PREC != PREC_COUNT) e = fminf(e, kEnergyCap);
             pol.store(w, lane, p, e);
         }

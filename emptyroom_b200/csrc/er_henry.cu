@@ -20,6 +20,8 @@
 
 namespace er {
 
+constexpr int kHenryP = 4;  // insertions per thread of the energy kernel
+
 struct BinGeom {
     int nb[3];  // bins per fractional axis
     int NB[3];  // 2x2x2 bricks per axis
@@ -134,10 +136,12 @@ __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_key
 __global__ void __launch_bounds__(kThreads, 2)
     henry_energy_kernel(const __grid_constant__ PointTask task) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if ((long long)blockIdx.x * (kWarps * 32 * kP) >= (long long)*task.n_valid) return;
+    if ((long long)blockIdx.x * (kWarps * 32 * kHenryP) >= (long long)*task.n_valid) return;
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
-    PointPolicy pol(&task, blockIdx.x);
-    process_cta<PointPolicy, PREC_COMP>(s, pol, task.fw, task.cc);
+    PointPolicy<kHenryP> pol(&task, blockIdx.x);
+    // near pairs in FP64: a Boltzmann factor turns an energy error dE into a
+    // relative weight error dE / T, so Widom energies get the tighter mode
+    process_cta<PointPolicy<kHenryP>, PREC_NEAR64>(s, pol, task.fw, task.cc);
 }
 
 __device__ __forceinline__ Lse lse_merge(Lse a, Lse b) {
@@ -195,29 +199,14 @@ __global__ void __launch_bounds__(256) henry_final_kernel(const Lse* __restrict_
     if (threadIdx.x == 0) *out = r;
 }
 
-}  // namespace er
 
-using namespace er;
-
-extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
-                        const uint8_t* block_mask, int mnx, int mny, int mnz,
-                        er_henry_result* out, float* energies_out) {
-    if (!ctx || !out) return ER_ERR_INVALID;
-    ER_CUDA(ctx, cudaSetDevice(ctx->device));
-    const FwRecord* f = find_fw(ctx, fw_id);
-    if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "henry: unknown framework id");
-    if (!(temperature > 0.0) || !std::isfinite(temperature))
-        return set_error(ctx, ER_ERR_INVALID, "henry: temperature must be positive");
-    if (n_ins < 1) return set_error(ctx, ER_ERR_INVALID, "henry: n_ins must be >= 1");
-    if (n_ins > (int64_t)INT32_MAX - 4096)
-        return set_error(ctx, ER_ERR_LIMIT, "henry: more than 2^31 - 4097 insertions per call");
-    if (block_mask && (mnx < 2 || mny < 2 || mnz < 2))
-        return set_error(ctx, ER_ERR_INVALID, "henry: mask dims must be >= 2");
-    const int n = (int)n_ins;
+int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, uint64_t seed,
+                  const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
+                  HenryScratch& hs, HenryOut* host_out) {
     // bins of ~16 expected points, shaped after the cell vector lengths
     BinGeom g;
     {
-        const double L0 = f->cell_len[0], L1 = f->cell_len[1], L2 = f->cell_len[2];
+        const double L0 = fw.cell_len[0], L1 = fw.cell_len[1], L2 = fw.cell_len[2];
         const double scale = cbrt((double)n / 16.0 / (L0 * L1 * L2));
         const double L[3] = {L0, L1, L2};
         int64_t nk = 8;
@@ -231,79 +220,124 @@ extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_in
         g.n_keys = (int)nk;
     }
     const size_t N = (size_t)n;
-    if (ctx->h_pts.ensure(3 * N * sizeof(double)) || ctx->h_bin.ensure(N * sizeof(int)) ||
-        ctx->h_order.ensure(N * sizeof(int)) || ctx->h_tmp.ensure(N * sizeof(int)) ||
-        ctx->h_counts.ensure(2 * (size_t)g.n_keys * sizeof(int)) ||
-        ctx->h_starts.ensure(((size_t)g.n_keys + 1) * sizeof(int)) ||
-        ctx->h_e.ensure(N * sizeof(float)) || ctx->h_nwt.ensure(4 * sizeof(int)) ||
-        ctx->h_part.ensure(4096 * sizeof(Lse)) || ctx->h_res.ensure(sizeof(Lse)))
+    if (hs.pts.ensure(3 * N * sizeof(double)) || hs.bin.ensure(N * sizeof(int)) ||
+        hs.order.ensure(N * sizeof(int)) || hs.tmp.ensure(N * sizeof(int)) ||
+        hs.counts.ensure(2 * (size_t)g.n_keys * sizeof(int)) ||
+        hs.starts.ensure(((size_t)g.n_keys + 1) * sizeof(int)) ||
+        hs.e.ensure(N * sizeof(float)) || hs.nblk.ensure(4 * sizeof(int)) ||
+        hs.part.ensure(4096 * sizeof(Lse)) || hs.res.ensure(sizeof(Lse)))
         return set_error(ctx, ER_ERR_NOMEM, "henry: device scratch allocation failed");
     const uint8_t* d_mask = nullptr;
     if (block_mask) {
-        const size_t mb = (size_t)mnx * mny * mnz;
-        if (ctx->h_mask.ensure(mb)) return set_error(ctx, ER_ERR_NOMEM, "henry: mask allocation");
-        ER_CUDA(ctx, cudaMemcpyAsync(ctx->h_mask.ptr, block_mask, mb, cudaMemcpyHostToDevice,
-                                     ctx->stream));
-        d_mask = (const uint8_t*)ctx->h_mask.ptr;
+        cudaPointerAttributes attr;
+        const bool on_device = cudaPointerGetAttributes(&attr, block_mask) == cudaSuccess &&
+                               attr.type == cudaMemoryTypeDevice;
+        cudaGetLastError();
+        if (on_device) {
+            d_mask = block_mask;  // e.g. the output of er_block_pockets_device
+        } else {
+            const size_t mb = (size_t)mnx * mny * mnz;
+            if (hs.mask.ensure(mb)) return set_error(ctx, ER_ERR_NOMEM, "henry: mask allocation");
+            ER_CUDA(ctx, cudaMemcpyAsync(hs.mask.ptr, block_mask, mb, cudaMemcpyHostToDevice, st));
+            d_mask = (const uint8_t*)hs.mask.ptr;
+        }
     }
-    int* counts = (int*)ctx->h_counts.ptr;
+    int* counts = (int*)hs.counts.ptr;
     int* fill = counts + g.n_keys;
-    int* starts = (int*)ctx->h_starts.ptr;
-    int* nblk = (int*)ctx->h_nwt.ptr;
-    float* E = (float*)ctx->h_e.ptr;
-    cudaStream_t st = ctx->stream;
+    int* starts = (int*)hs.starts.ptr;
+    int* nblk = (int*)hs.nblk.ptr;
+    float* E = (float*)hs.e.ptr;
     ER_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * (size_t)g.n_keys * sizeof(int), st));
     ER_CUDA(ctx, cudaMemsetAsync(nblk, 0, sizeof(int), st));
     const int gthreads = 256;
     const int gblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads,
                                                (int64_t)ctx->num_sms * 32);
     henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
-                                                   (double*)ctx->h_pts.ptr, (int*)ctx->h_bin.ptr,
-                                                   counts, E, nblk);
+                                                   (double*)hs.pts.ptr, (int*)hs.bin.ptr, counts,
+                                                   E, nblk);
     scan_kernel<<<1, 1024, 0, st>>>(counts, starts, g.n_keys);
-    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)ctx->h_bin.ptr, n, starts,
-                                                       fill, (int*)ctx->h_tmp.ptr);
+    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, n, starts, fill,
+                                                       (int*)hs.tmp.ptr);
     henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
-                                                              (const int*)ctx->h_tmp.ptr,
-                                                              (int*)ctx->h_order.ptr);
+                                                              (const int*)hs.tmp.ptr,
+                                                              (int*)hs.order.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     PointTask task;
-    task.fw = f->dev;
-    task.cc = make_cutoff_consts(f->rc2, 0.0, 1e-16 * 1e-16);  // min_r, src/doHenry.h:15
-    task.pts = (const double*)ctx->h_pts.ptr;
-    task.order = (const int*)ctx->h_order.ptr;
+    task.fw = fw.dev;
+    task.cc = make_cutoff_consts(fw.rc2, 0.0, 1e-16 * 1e-16);  // min_r, src/doHenry.h:15
+    task.pts = (const double*)hs.pts.ptr;
+    task.order = (const int*)hs.order.ptr;
     task.n_valid = starts + g.n_keys;
     task.energies = E;
     ER_CUDA(ctx, cudaFuncSetAttribute(henry_energy_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(EngineSmem)));
-    const int per_cta = kWarps * 32 * kP;
+    const int per_cta = kWarps * 32 * kHenryP;
     const int ecta = (n + per_cta - 1) / per_cta;
     henry_energy_kernel<<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
     ER_CUDA(ctx, cudaGetLastError());
     const int rblocks = std::min(4096, std::max(1, ctx->num_sms * 4));
     const int chunk = (n + rblocks - 1) / rblocks;
     const int nrb = (n + chunk - 1) / chunk;
-    henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, temperature, chunk, (Lse*)ctx->h_part.ptr);
-    henry_final_kernel<<<1, 256, 0, st>>>((const Lse*)ctx->h_part.ptr, nrb, (Lse*)ctx->h_res.ptr);
+    henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, temperature, chunk, (Lse*)hs.part.ptr);
+    henry_final_kernel<<<1, 256, 0, st>>>((const Lse*)hs.part.ptr, nrb, (Lse*)hs.res.ptr);
     ER_CUDA(ctx, cudaGetLastError());
-    Lse r;
-    int nb_host = 0;
-    ER_CUDA(ctx, cudaMemcpyAsync(&r, ctx->h_res.ptr, sizeof(Lse), cudaMemcpyDeviceToHost, st));
-    ER_CUDA(ctx, cudaMemcpyAsync(&nb_host, nblk, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (energies_out)
-        ER_CUDA(ctx, cudaMemcpyAsync(energies_out, E, N * sizeof(float), cudaMemcpyDeviceToHost,
-                                     st));
-    ER_CUDA(ctx, cudaStreamSynchronize(st));
-    out->log_scale = r.m;
-    out->sum_w_scaled = r.s;
-    out->sum_ew_scaled = r.se;
-    out->sum_w = r.s > 0 ? r.s * exp(r.m) : 0.0;
-    out->sum_ew = r.s > 0 ? r.se * exp(r.m) : 0.0;
+    if (host_out) {
+        ER_CUDA(ctx, cudaMemcpyAsync(host_out->lse, hs.res.ptr, sizeof(Lse),
+                                     cudaMemcpyDeviceToHost, st));
+        ER_CUDA(ctx, cudaMemcpyAsync(&host_out->n_blocked, nblk, sizeof(int),
+                                     cudaMemcpyDeviceToHost, st));
+    }
+    return ER_OK;
+}
+
+void henry_finish(const HenryOut& h, int64_t n, double temperature, er_henry_result* out) {
+    const double m = h.lse[0], s = h.lse[1], se = h.lse[2];
+    out->log_scale = m;
+    out->sum_w_scaled = s;
+    out->sum_ew_scaled = se;
+    out->sum_w = s > 0 ? s * exp(m) : 0.0;
+    out->sum_ew = s > 0 ? se * exp(m) : 0.0;
     out->n_insertions = (double)n;
-    out->n_blocked = (double)nb_host;
-    out->mean_energy = r.s > 0 ? r.se / r.s : 0.0;
+    out->n_blocked = (double)h.n_blocked;
+    out->mean_energy = s > 0 ? se / s : 0.0;
     // K_H = sum w / N / T / 8.314 (mol/(m^3 Pa)), src/henry.cu:169
     out->kh_mol_m3_pa = out->sum_w / (double)n / temperature / 8.314;
+}
+
+int henry_check(er_ctx* ctx, double temperature, int64_t n_ins, const uint8_t* block_mask,
+                int mnx, int mny, int mnz) {
+    if (!(temperature > 0.0) || !std::isfinite(temperature))
+        return set_error(ctx, ER_ERR_INVALID, "henry: temperature must be positive");
+    if (n_ins < 1) return set_error(ctx, ER_ERR_INVALID, "henry: n_ins must be >= 1");
+    if (n_ins > (int64_t)INT32_MAX - 4096)
+        return set_error(ctx, ER_ERR_LIMIT, "henry: more than 2^31 - 4097 insertions per call");
+    if (block_mask && (mnx < 2 || mny < 2 || mnz < 2))
+        return set_error(ctx, ER_ERR_INVALID, "henry: mask dims must be >= 2");
+    return ER_OK;
+}
+
+}  // namespace er
+
+using namespace er;
+
+extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
+                        const uint8_t* block_mask, int mnx, int mny, int mnz,
+                        er_henry_result* out, float* energies_out) {
+    if (!ctx || !out) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    const FwRecord* f = find_fw(ctx, fw_id);
+    if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "henry: unknown framework id");
+    int st = henry_check(ctx, temperature, n_ins, block_mask, mnx, mny, mnz);
+    if (st != ER_OK) return st;
+    HenryOut h;
+    st = henry_enqueue(ctx, *f, temperature, (int)n_ins, seed, block_mask, mnx, mny, mnz,
+                       ctx->stream, ctx->henry, &h);
+    if (st != ER_OK) return st;
+    if (energies_out)
+        ER_CUDA(ctx, cudaMemcpyAsync(energies_out, ctx->henry.e.ptr, (size_t)n_ins * sizeof(float),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    henry_finish(h, n_ins, temperature, out);
     return ER_OK;
 }

@@ -80,6 +80,13 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
         }
         f.atom_frac[a] = HostImage{p.x_f, p.y_f, p.z_f, p.sig_with_adsorbate_squared};
     }
+    f.atom_lj64.resize(2 * (size_t)d.n_atoms);
+    for (int a = 0; a < d.n_atoms; ++a) {
+        const double s2 = d.atoms[a].sig_with_adsorbate_squared;
+        const double c6 = 4.0 * d.atoms[a].eps_with_adsorbate * s2 * s2 * s2;
+        f.atom_lj64[2 * a] = c6 * s2 * s2 * s2;
+        f.atom_lj64[2 * a + 1] = c6;
+    }
     // Keep image a + n only if it can be within rc of the grid region
     // [0,1]^3: its fractional overshoot of slab d times the slab width w_d is a
     // lower bound on its distance to every grid point.

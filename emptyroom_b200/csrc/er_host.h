@@ -28,6 +28,7 @@ struct HostFramework {
     std::vector<uint32_t> img_id;       // atom * imgs_per_atom + image code
     std::vector<int> cell_start;        // nc0*nc1*nc2 + 1
     std::vector<HostImage> atom_frac;   // x_f, y_f, z_f, sig2 per atom
+    std::vector<double> atom_lj64;      // 2 per atom: C12, C6 in FP64
 };
 
 // Validates desc and builds the image cell list with cell edge h (A).

@@ -18,6 +18,7 @@ struct FwDev {
     const uint32_t* img_id;   // atom * imgs_per_atom + image code
     const int* cell_start;    // nc0*nc1*nc2 + 1 offsets into the image arrays
     const double4* atom_frac; // FP64 fractional (x_f, y_f, z_f, sig2) per atom
+    const double2* atom_lj64; // FP64 (C12, C6) per atom (near pairs of PREC_NEAR64)
     int n_img;
     int n_atoms;
     int nc[3];                // cells per axis
@@ -45,6 +46,7 @@ struct GridTask {
     CutoffConsts cc;
     int nx, ny, nz;
     int nb[3];          // bricks per axis
+    int tile_p;         // points per thread of the kernel variant (brick 2P x 8 x 16)
     float* out;         // nx*ny*nz, index k + j*nz + i*ny*nz
 };
 

@@ -473,6 +473,102 @@ extern "C" int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, i
     return ER_OK;
 }
 
-extern "C" int er_accessibility(er_ctx* ctx, int, int, int, int, uint8_t*) {
-    return er::set_error(ctx, ER_ERR_INVALID, "er_accessibility: not available in this build");
+// ------------------------------------------------------------------ accessibility
+// ComputeGridSheetAccessibleOrNot (src/computegridsheet.h:101-165): a point is
+// inaccessible (0) when some atom image within +-1 cells has r^2 < sigma_mix^2.
+// Image positions and r^2 follow the reference's FP64 expressions without
+// contraction, so the mask is bit-exact.
+namespace er {
+
+struct AccParams {
+    double t[9];
+    int nx, ny, nz;
+};
+
+__device__ __forceinline__ void acc_cart(const double* t, double xf, double yf, double zf,
+                                         double& x, double& y, double& z) {
+    x = __dadd_rn(__dadd_rn(__dmul_rn(t[0], xf), __dmul_rn(t[1], yf)), __dmul_rn(t[2], zf));
+    y = __dadd_rn(__dadd_rn(__dmul_rn(t[3], xf), __dmul_rn(t[4], yf)), __dmul_rn(t[5], zf));
+    z = __dadd_rn(__dadd_rn(__dmul_rn(t[6], xf), __dmul_rn(t[7], yf)), __dmul_rn(t[8], zf));
+}
+
+__global__ void acc_images_kernel(const double4* __restrict__ atoms, int n, AccParams P,
+                                  double4* __restrict__ img) {
+    const int total = 27 * n;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int a = q / 27, m = q % 27;
+        const int i = m / 9 - 1, j = (m / 3) % 3 - 1, k = m % 3 - 1;
+        const double4 at = atoms[a];
+        double x, y, z;
+        // src/computegridsheet.h:134-140
+        acc_cart(P.t, __dadd_rn(at.x, (double)i), __dadd_rn(at.y, (double)j),
+                 __dadd_rn(at.z, (double)k), x, y, z);
+        img[q] = make_double4(x, y, z, at.w);
+    }
+}
+
+__global__ void __launch_bounds__(256) acc_grid_kernel(const double4* __restrict__ img, int nimg,
+                                                       AccParams P, uint8_t* __restrict__ out) {
+    __shared__ double4 tile[512];
+    const int64_t n = (int64_t)P.nx * P.ny * P.nz;
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double x = 0, y = 0, z = 0;
+    bool live = p < n, overlap = false;
+    if (live) {
+        const int k = (int)(p % P.nz), j = (int)((p / P.nz) % P.ny),
+                  i = (int)(p / ((int64_t)P.ny * P.nz));
+        acc_cart(P.t, __ddiv_rn((double)i, (double)(P.nx - 1)),
+                 __ddiv_rn((double)j, (double)(P.ny - 1)),
+                 __ddiv_rn((double)k, (double)(P.nz - 1)), x, y, z);
+    }
+    for (int base = 0; base < nimg; base += 512) {
+        const int cnt = min(512, nimg - base);
+        __syncthreads();
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x) tile[q] = img[base + q];
+        __syncthreads();
+        if (live && !overlap) {
+            for (int q = 0; q < cnt; ++q) {
+                const double4 w = tile[q];
+                const double dx = __dsub_rn(x, w.x), dy = __dsub_rn(y, w.y),
+                             dz = __dsub_rn(z, w.z);
+                const double r2 =
+                    __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                if (r2 < w.w) {  // src/computegridsheet.h:148
+                    overlap = true;
+                    break;
+                }
+            }
+        }
+    }
+    if (live) out[p] = overlap ? 0 : 1;
+}
+
+}  // namespace er
+
+extern "C" int er_accessibility(er_ctx* ctx, int fw_id, int nx, int ny, int nz, uint8_t* out) {
+    if (!ctx || !out) return ER_ERR_INVALID;
+    if (nx < 2 || ny < 2 || nz < 2)
+        return er::set_error(ctx, ER_ERR_INVALID, "accessibility: nx, ny, nz must be >= 2");
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    const er::FwRecord* f = er::find_fw(ctx, fw_id);
+    if (!f) return er::set_error(ctx, ER_ERR_NOT_FOUND, "accessibility: unknown framework id");
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int nimg = 27 * f->n_atoms;
+    if (ctx->p_lab.ensure(std::max<size_t>((size_t)nimg, 1) * sizeof(double4)) ||
+        ctx->p_seg.ensure((size_t)n))
+        return er::set_error(ctx, ER_ERR_NOMEM, "accessibility: scratch allocation failed");
+    er::AccParams P;
+    for (int k = 0; k < 9; ++k) P.t[k] = f->t[k];
+    P.nx = nx; P.ny = ny; P.nz = nz;
+    cudaStream_t st = ctx->stream;
+    double4* img = (double4*)ctx->p_lab.ptr;
+    if (nimg > 0)
+        er::acc_images_kernel<<<std::max(1, std::min((nimg + 255) / 256, ctx->num_sms * 8)), 256,
+                                0, st>>>(f->dev.atom_frac, f->n_atoms, P, img);
+    er::acc_grid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(img, nimg, P,
+                                                                     (uint8_t*)ctx->p_seg.ptr);
+    ER_CUDA(ctx, cudaGetLastError());
+    ER_CUDA(ctx, cudaMemcpyAsync(out, ctx->p_seg.ptr, (size_t)n, cudaMemcpyDeviceToHost, st));
+    ER_CUDA(ctx, cudaStreamSynchronize(st));
+    return ER_OK;
 }

@@ -1,0 +1,398 @@
+// er_server.cu -- request server with continuous batching (er_server_*).
+//
+// One scheduler thread per server. Jobs wait in arrival order; the head job
+// is admitted when a slot (a CUDA stream with its own Widom scratch) is free
+// and its device footprint fits the HBM budget after evicting unpinned cached
+// grids (least recently used first). An admitted job's kernels go onto its
+// slot's stream at once, so the device runs the kernels of every admitted job
+// concurrently and new arrivals join while earlier ones are still running.
+// Completion is detected with one event per slot. Frameworks (the image cell
+// lists) and finished grids stay resident and are reused by later jobs.
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "er_ctx.h"
+#include "er_engine.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+using GridKey = std::tuple<uint64_t, int, int, int>;
+
+struct SrvFw {
+    int fw_id = 0;
+    size_t bytes = 0;
+    uint64_t last_use = 0;
+    int pins = 0;
+};
+
+struct SrvGrid {
+    float* ptr = nullptr;
+    size_t bytes = 0;
+    uint64_t last_use = 0;
+    int pins = 0;
+    bool ready = false;
+};
+
+struct SrvJob {
+    er_job job{};
+    er_job_status st{};
+    int slot = -1;
+    GridKey gkey{};
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    er::HenryScratch hs;
+    er::HenryOut* pinned = nullptr;  // host copy of the Widom reduction
+    uint64_t ticket = 0;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct er_server {
+    er_ctx* ctx = nullptr;
+    size_t budget = 0;
+    std::vector<Slot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint64_t> pending;
+    std::unordered_map<uint64_t, SrvJob> jobs;
+    std::unordered_map<uint64_t, SrvFw> fws;
+    std::map<GridKey, SrvGrid> grids;
+    size_t bytes_fw = 0, bytes_grid = 0;
+    uint64_t next_ticket = 1, tick = 0;
+    bool stop = false;
+    std::thread thr;
+    Clock::time_point t0;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+    size_t scratch_bytes() const {
+        size_t b = 0;
+        for (const Slot& s : slots) b += s.hs.bytes();
+        return b;
+    }
+    size_t used() const { return bytes_fw + bytes_grid + scratch_bytes(); }
+
+    // Frees least recently used grids that no running job holds until
+    // `need` more bytes fit the budget; returns whether they fit.
+    bool make_room(size_t need, cudaStream_t st) {
+        while (used() + need > budget) {
+            auto victim = grids.end();
+            for (auto it = grids.begin(); it != grids.end(); ++it)
+                if (it->second.pins == 0 && it->second.ready &&
+                    (victim == grids.end() || it->second.last_use < victim->second.last_use))
+                    victim = it;
+            if (victim == grids.end()) return false;
+            cudaFreeAsync(victim->second.ptr, st);
+            bytes_grid -= victim->second.bytes;
+            grids.erase(victim);
+        }
+        return true;
+    }
+
+    void finish(SrvJob& j, int status) {
+        j.st.done = 1;
+        j.st.status = status;
+        j.st.finish_s = now();
+    }
+
+    // Returns true when the head job was admitted or resolved.
+    bool admit_one() {
+        if (pending.empty()) return false;
+        int free_slot = -1;
+        for (size_t i = 0; i < slots.size(); ++i)
+            if (!slots[i].busy) {
+                free_slot = (int)i;
+                break;
+            }
+        if (free_slot < 0) return false;
+        const uint64_t ticket = pending.front();
+        SrvJob& j = jobs[ticket];
+        Slot& sl = slots[free_slot];
+        const er_job& job = j.job;
+        ++tick;
+        // a grid that is already resident completes at once
+        if (job.kind == ER_JOB_GRID) {
+            j.gkey = GridKey(job.fw_key, job.nx, job.ny, job.nz);
+            auto g = grids.find(j.gkey);
+            if (g != grids.end() && g->second.ready) {
+                g->second.last_use = tick;
+                j.st.grid_cache_hit = 1;
+                j.st.start_s = now();
+                if (job.grid_out_host)
+                    cudaMemcpy(job.grid_out_host, g->second.ptr, g->second.bytes,
+                               cudaMemcpyDeviceToHost);
+                finish(j, ER_OK);
+                pending.pop_front();
+                cv_done.notify_all();
+                return true;
+            }
+        }
+        // framework resident?
+        auto f = fws.find(job.fw_key);
+        if (f == fws.end()) {
+            if (!job.desc) {
+                pending.pop_front();
+                finish(j, ER_ERR_NOT_FOUND);
+                cv_done.notify_all();
+                return true;
+            }
+            int fw_id = 0;
+            int st = er_framework_upload(ctx, job.desc, &fw_id);
+            if (st != ER_OK) {
+                pending.pop_front();
+                finish(j, st);
+                cv_done.notify_all();
+                return true;
+            }
+            SrvFw rec;
+            rec.fw_id = fw_id;
+            er_framework_bytes(ctx, fw_id, &rec.bytes);
+            bytes_fw += rec.bytes;
+            f = fws.emplace(job.fw_key, rec).first;
+        }
+        const er::FwRecord* fr = er::find_fw(ctx, f->second.fw_id);
+        // footprint
+        size_t need = 0;
+        if (job.kind == ER_JOB_GRID) {
+            need = (size_t)job.nx * job.ny * job.nz * sizeof(float);
+        } else {
+            const size_t want = (size_t)job.n_insertions * 41 + (4u << 20);
+            const size_t have = sl.hs.bytes();
+            need = want > have ? want - have : 0;
+        }
+        if (!make_room(need, sl.stream)) {
+            // nothing left to evict: wait for running jobs, or fail if none run
+            bool any_busy = false;
+            for (const Slot& s : slots) any_busy |= s.busy;
+            if (any_busy) return false;
+            pending.pop_front();
+            finish(j, ER_ERR_NOMEM);
+            cv_done.notify_all();
+            return true;
+        }
+        f->second.last_use = tick;
+        f->second.pins++;
+        j.st.start_s = now();
+        int st = ER_OK;
+        if (job.kind == ER_JOB_GRID) {
+            SrvGrid g;
+            g.bytes = need;
+            if (cudaMallocAsync((void**)&g.ptr, g.bytes, sl.stream) != cudaSuccess) {
+                cudaGetLastError();
+                st = ER_ERR_NOMEM;
+            } else {
+                er::GridTask t;
+                st = er::fill_grid_task(ctx, *fr, job.nx, job.ny, job.nz, g.ptr, t);
+                if (st == ER_OK) st = er::launch_grid_plain_on(ctx, t, er::PREC_COMP, sl.stream);
+                if (st == ER_OK && job.grid_out_host &&
+                    cudaMemcpyAsync(job.grid_out_host, g.ptr, g.bytes, cudaMemcpyDeviceToHost,
+                                    sl.stream) != cudaSuccess) {
+                    cudaGetLastError();
+                    st = ER_ERR_CUDA;
+                }
+                if (st == ER_OK) {
+                    g.pins = 1;
+                    g.last_use = tick;
+                    bytes_grid += g.bytes;
+                    grids[j.gkey] = g;
+                } else {
+                    cudaFreeAsync(g.ptr, sl.stream);
+                }
+            }
+        } else {
+            st = er::henry_check(ctx, job.temperature, job.n_insertions, nullptr, 0, 0, 0);
+            if (st == ER_OK)
+                st = er::henry_enqueue(ctx, *fr, job.temperature, (int)job.n_insertions, job.seed,
+                                       nullptr, 0, 0, 0, sl.stream, sl.hs, sl.pinned);
+        }
+        pending.pop_front();
+        if (st != ER_OK) {
+            f->second.pins--;
+            finish(j, st);
+            cv_done.notify_all();
+            return true;
+        }
+        cudaEventRecord(sl.done, sl.stream);
+        sl.busy = true;
+        sl.ticket = ticket;
+        j.slot = free_slot;
+        return true;
+    }
+
+    bool reap() {
+        bool any = false;
+        for (Slot& sl : slots) {
+            if (!sl.busy) continue;
+            const cudaError_t q = cudaEventQuery(sl.done);
+            if (q == cudaErrorNotReady) continue;
+            SrvJob& j = jobs[sl.ticket];
+            int status = ER_OK;
+            if (q != cudaSuccess) {
+                cudaGetLastError();
+                status = ER_ERR_CUDA;
+            }
+            if (j.job.kind == ER_JOB_HENRY && status == ER_OK)
+                er::henry_finish(*sl.pinned, j.job.n_insertions, j.job.temperature, &j.st.henry);
+            if (j.job.kind == ER_JOB_GRID) {
+                auto g = grids.find(j.gkey);
+                if (g != grids.end()) {
+                    g->second.pins--;
+                    g->second.ready = status == ER_OK;
+                }
+            }
+            auto f = fws.find(j.job.fw_key);
+            if (f != fws.end()) f->second.pins--;
+            finish(j, status);
+            sl.busy = false;
+            any = true;
+        }
+        if (any) cv_done.notify_all();
+        return any;
+    }
+
+    void run() {
+        cudaSetDevice(ctx->device);
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            bool progress = reap();
+            while (!stop && admit_one()) progress = true;
+            bool busy = false;
+            for (const Slot& s : slots) busy |= s.busy;
+            if (stop && !busy) break;
+            if (!progress) cv_work.wait_for(lk, std::chrono::microseconds(busy ? 20 : 2000));
+        }
+    }
+};
+
+using namespace er;
+
+extern "C" {
+
+int er_server_create(er_ctx* ctx, size_t hbm_budget_bytes, int slots, er_server** out) {
+    if (!ctx || !out || slots < 1 || slots > 64 || hbm_budget_bytes == 0) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    er_server* s = new er_server();
+    s->ctx = ctx;
+    s->budget = hbm_budget_bytes;
+    s->t0 = Clock::now();
+    s->slots.resize(slots);
+    for (Slot& sl : s->slots) {
+        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost((void**)&sl.pinned, sizeof(HenryOut)) != cudaSuccess) {
+            cudaGetLastError();
+            er_server_destroy(s);
+            return set_error(ctx, ER_ERR_CUDA, "server: stream/event creation failed");
+        }
+    }
+    s->thr = std::thread([s]() { s->run(); });
+    *out = s;
+    return ER_OK;
+}
+
+int er_server_submit(er_server* s, const er_job* job, uint64_t* ticket) {
+    if (!s || !job || !ticket) return ER_ERR_INVALID;
+    if (job->kind != ER_JOB_GRID && job->kind != ER_JOB_HENRY) return ER_ERR_INVALID;
+    if (job->kind == ER_JOB_GRID && (job->nx < 2 || job->ny < 2 || job->nz < 2))
+        return ER_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return ER_ERR_INVALID;
+    const uint64_t t = s->next_ticket++;
+    SrvJob j;
+    j.job = *job;
+    j.st.submit_s = s->now();
+    s->jobs.emplace(t, j);
+    s->pending.push_back(t);
+    *ticket = t;
+    s->cv_work.notify_one();
+    return ER_OK;
+}
+
+int er_server_poll(er_server* s, uint64_t ticket, er_job_status* st) {
+    if (!s || !st) return ER_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return ER_ERR_NOT_FOUND;
+    *st = it->second.st;
+    return ER_OK;
+}
+
+int er_server_wait(er_server* s, uint64_t ticket, double timeout_s, er_job_status* st) {
+    if (!s || !st || !(timeout_s >= 0)) return ER_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return ER_ERR_NOT_FOUND;
+    const auto until = Clock::now() + std::chrono::duration<double>(timeout_s);
+    while (!s->jobs[ticket].st.done) {
+        if (s->cv_done.wait_until(lk, until) == std::cv_status::timeout &&
+            !s->jobs[ticket].st.done) {
+            *st = s->jobs[ticket].st;
+            return ER_ERR_TIMEOUT;
+        }
+    }
+    *st = s->jobs[ticket].st;
+    return ER_OK;
+}
+
+int er_server_grid(er_server* s, uint64_t ticket, const float** grid) {
+    if (!s || !grid) return ER_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end() || it->second.job.kind != ER_JOB_GRID || !it->second.st.done)
+        return ER_ERR_NOT_FOUND;
+    auto g = s->grids.find(it->second.gkey);
+    if (g == s->grids.end() || !g->second.ready) return ER_ERR_NOT_FOUND;
+    *grid = g->second.ptr;
+    return ER_OK;
+}
+
+double er_server_now(const er_server* s) { return s ? s->now() : 0.0; }
+
+int er_server_bytes(const er_server* s, size_t* bytes) {
+    if (!s || !bytes) return ER_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(const_cast<er_server*>(s)->mu);
+    *bytes = s->used();
+    return ER_OK;
+}
+
+void er_server_destroy(er_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        for (uint64_t t : s->pending) s->finish(s->jobs[t], ER_ERR_INVALID);
+        s->pending.clear();
+        s->cv_work.notify_all();
+        s->cv_done.notify_all();
+    }
+    if (s->thr.joinable()) s->thr.join();
+    cudaSetDevice(s->ctx->device);
+    for (Slot& sl : s->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        sl.hs.release();
+        if (sl.pinned) cudaFreeHost(sl.pinned);
+        if (sl.done) cudaEventDestroy(sl.done);
+    }
+    for (auto& kv : s->grids) cudaFree(kv.second.ptr);
+    for (auto& kv : s->fws) er_framework_release(s->ctx, kv.second.fw_id);
+    for (Slot& sl : s->slots)
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    delete s;
+}
+
+}  // extern "C"

@@ -84,10 +84,15 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);
 #define ER_OUT_F32 0x0       /* float per point */
 #define ER_OUT_F64 0x2       /* double per point (the reference's sheet type) */
 #define ER_PREC_COMP 0x0     /* FP32 pair terms, compensated (two-float) accumulation */
+#define ER_PREC_NEAR64 0x08  /* as ER_PREC_COMP, with the pairs of atoms within 5 A of
+                                a warp's points in FP64 (the default of er_henry) */
 #define ER_PREC_FP32 0x10    /* FP32 pair terms, plain FP32 accumulation */
 #define ER_PREC_FP64 0x20    /* FP64 pair terms and accumulation (precision sweeps) */
 #define ER_COUNT_PAIRS 0x40  /* diagnostic: write the number of in-cutoff pair terms per
                                 point instead of the energy (same traversal) */
+#define ER_TILE_P8 0x80      /* kernel variant with 8 points per thread (16 x 8 x 16
+                                bricks) instead of 4; results agree within the FP32
+                                tolerance, not bit for bit */
 
 /* Energies above this value (K) are written as this value (overflow cap). */
 #define ER_ENERGY_CAP 1.0e30
@@ -120,6 +125,11 @@ typedef struct {
 #define ER_BATCH_PLAIN 1      /* one plain launch per job, in order */
 #define ER_BATCH_HOST_OUT 0x100 /* or-ed into mode: out_device fields are host pointers;
                                    grids are staged on the device and copied back */
+#define ER_BATCH_AUTOTUNE 0x200 /* or-ed into mode: pick each job's kernel variant (4 or
+                                   8 points per thread) by timing both on a sample of the
+                                   first job of its class (atom density, grid spacing,
+                                   cutoff); choices are cached in the context. A job's
+                                   result then equals er_grid with that variant's flag. */
 
 /* Runs many grid jobs (uneven frameworks, probes, grid sizes). Results are
  * identical between the two modes and independent of the job mix. */
@@ -132,6 +142,9 @@ int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int m
 int er_batch_plan_run(er_batch_plan* plan); /* asynchronous on the context stream */
 /* Kernel launches one run of the plan issues (its CUDA graph's kernel nodes). */
 int er_batch_plan_launches(const er_batch_plan* plan, int* n_launches);
+/* Points per thread (4 or 8) of the kernel variant the plan uses for job `job`
+ * (8: reproduce with ER_TILE_P8 in er_grid). */
+int er_batch_plan_tile(const er_batch_plan* plan, int job, int* tile_p);
 void er_batch_plan_destroy(er_batch_plan* plan);
 
 /* ------------------------------------------------------------------ Widom / Henry */
@@ -150,9 +163,10 @@ typedef struct {
 /* Widom insertions i = 0..n_ins-1 at Philox4x32-10 points of stream `seed`
  * (fractional coordinates uniform in [0,1), 53 bits each), E by the pair sum
  * of src/doHenry.h:70-98, FP64 log-sum-exp reduction of
- * src/doHenry.h:106-125 and src/henry.cu:157-169. block_mask (host, may be
- * NULL) is an mnx x mny x mnz grid (axes i/(N-1)); an insertion whose 8
- * surrounding corners include a set entry is blocked and has weight 0.
+ * src/doHenry.h:106-125 and src/henry.cu:157-169. block_mask (host or device
+ * memory, may be NULL) is an mnx x mny x mnz grid (axes i/(N-1)), e.g. the
+ * pocket mask of er_block_pockets_device; an insertion whose 8 surrounding
+ * corners include a set entry is blocked and has weight 0.
  * energies_out (host, may be NULL) receives E per insertion as float. */
 int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
              const uint8_t* block_mask, int mnx, int mny, int mnz, er_henry_result* out,
@@ -216,6 +230,56 @@ void er_insertion_point(uint64_t seed, uint64_t i, double out[3]);
  * be reached within the attempt budget. */
 int er_synth_positions(uint64_t seed, const double t_matrix[9], int n_atoms, double d_min,
                        double* frac_out);
+
+/* ------------------------------------------------------------------ serving */
+/* A request server over one context: jobs are submitted from any host thread
+ * as they arrive; a scheduler thread admits them in arrival order while a job
+ * slot is free and their device footprint fits the HBM budget, and launches
+ * each admitted job on its slot's stream, so jobs that arrive while others
+ * run execute concurrently on the device (continuous batching). Framework
+ * images and finished grids stay resident on the device (caches keyed by the
+ * caller's framework key and the grid size); least recently used grids are
+ * evicted when the budget needs room. A job's result does not depend on which
+ * other jobs run beside it. With slots = 1 the server runs one job at a time
+ * (the plain one-job-per-launch loop). The reference has no serving layer. */
+typedef struct er_server er_server;
+#define ER_JOB_GRID 1
+#define ER_JOB_HENRY 2
+typedef struct {
+    int kind;                        /* ER_JOB_GRID or ER_JOB_HENRY */
+    uint64_t fw_key;                 /* caller's key of the framework/probe pair */
+    const er_framework_desc* desc;   /* read (host) when fw_key is not resident yet;
+                                        must stay valid until the job completes */
+    int nx, ny, nz;                  /* grid jobs */
+    double temperature;              /* Henry jobs */
+    int64_t n_insertions;
+    uint64_t seed;
+    float* grid_out_host;            /* optional host copy of the grid (pinned memory
+                                        keeps the copy asynchronous) */
+} er_job;
+typedef struct {
+    int done;                        /* 1 once finished (status holds the outcome) */
+    int status;                      /* er_status of the job */
+    int grid_cache_hit;              /* the grid was already resident */
+    double submit_s, start_s, finish_s; /* server clock, seconds */
+    er_henry_result henry;           /* Henry jobs */
+} er_job_status;
+int er_server_create(er_ctx* ctx, size_t hbm_budget_bytes, int slots, er_server** out);
+/* Thread-safe; returns at once with a ticket (>= 1). */
+int er_server_submit(er_server* s, const er_job* job, uint64_t* ticket);
+/* Copies the job's status; ER_ERR_NOT_FOUND for an unknown ticket. */
+int er_server_poll(er_server* s, uint64_t ticket, er_job_status* st);
+/* Waits up to timeout_s for the job; ER_ERR_TIMEOUT when it is still running. */
+int er_server_wait(er_server* s, uint64_t ticket, double timeout_s, er_job_status* st);
+/* Device pointer of a finished grid job's resident grid (valid until that
+ * grid is evicted or the server is destroyed). */
+int er_server_grid(er_server* s, uint64_t ticket, const float** grid);
+/* Server clock (seconds), the clock of er_job_status. */
+double er_server_now(const er_server* s);
+/* Device bytes held by resident frameworks, grids and job scratch. */
+int er_server_bytes(const er_server* s, size_t* bytes);
+/* Drains running jobs and frees everything the server holds. */
+void er_server_destroy(er_server* s);
 
 /* ------------------------------------------------------------------ file formats */
 /* The reference's input files, read the way its loaders read them. Paths are

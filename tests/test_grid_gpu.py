@@ -211,3 +211,65 @@ def test_batch_matches_oracle_sampled(ctx):
         S = oracle.points_abs(f.particles(), f.t_matrix, f.rep, f.rc2, pts, 1e-12)
         got = o.cpu().numpy()[idx[:, 0], idx[:, 1], idx[:, 2]]
         _check(grid_errors(got, ref, S))
+
+
+@pytest.mark.parametrize("name", ["grid_cubic", "grid_triclinic", "grid_rep2"])
+def test_accessibility_matches_golden(ctx, name):
+    g = golden(name)
+    fw = ctx.upload(g["particles"], g["t_matrix"], g["rep"], float(g["rc2"]))
+    a = ctx.accessibility(fw, g["dims"])
+    assert np.array_equal(a, g["accessibility"])
+
+
+def test_accessibility_matches_oracle_config1(ctx):
+    f = synth.config1(9)
+    P = f.particles()
+    P[::7, 3] = 0.0  # epsilon = 0 atoms still occupy space in the hard-sphere test
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    a = ctx.accessibility(fw, (40, 33, 29))
+    assert np.array_equal(a, oracle.accessibility(P, f.t_matrix, (40, 33, 29)))
+
+
+def test_autotuned_plan_matches_er_grid_with_its_variant(ctx):
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=8, seed=140)
+    outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    plan = ctx.batch_plan([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)],
+                          er.ER_BATCH_PERSISTENT | er.ER_BATCH_AUTOTUNE)
+    plan.run()
+    ctx.synchronize()
+    for k, (u, f, o) in enumerate(zip(ups, fws, outs)):
+        p = plan.tile(k)
+        assert p in (4, 8)
+        flags = er.ER_TILE_P8 if p == 8 else 0
+        assert np.array_equal(o.cpu().numpy(), ctx.grid(u, f.dims, precision=flags))
+    plan.close()
+
+
+@pytest.mark.parametrize("flags", [er.ER_TILE_P8, er.ER_PREC_NEAR64,
+                                   er.ER_PREC_NEAR64 | er.ER_TILE_P8])
+def test_variants_match_oracle(ctx, flags):
+    f = synth.make_framework(150, (17.0, 19.0, 18.0), (80, 100, 95), 120, probe="Xe")
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    dims = (27, 19, 33)
+    e = ctx.grid(fw, dims, precision=flags)
+    ref = oracle.grid(P, f.t_matrix, f.rep, f.rc2, dims)
+    S = oracle.grid_abs(P, f.t_matrix, f.rep, f.rc2, dims)
+    _check(grid_errors(e, ref, S))
+
+
+def test_near64_is_more_accurate(ctx):
+    f = synth.config1(7)
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    dims = (30, 30, 30)
+    ref = oracle.grid(P, f.t_matrix, f.rep, f.rc2, dims)
+    neg = ref < 0
+    e32 = ctx.grid(fw, dims).astype(np.float64)
+    e64 = ctx.grid(fw, dims, precision=er.ER_PREC_NEAR64).astype(np.float64)
+    err32 = np.abs(e32 - ref)[neg].max()
+    err64 = np.abs(e64 - ref)[neg].max()
+    # NEAR64 errors are left by the FP32 far pairs and the FP32 output rounding
+    assert err64 < err32
+    assert np.all(np.abs(e64 - ref)[neg] <= 2e-6 * np.abs(ref[neg]) + 2e-4)

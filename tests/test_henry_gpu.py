@@ -101,3 +101,27 @@ def test_henry_invalid(ctx):
         ctx.henry(fw, -1.0, 100, seed=0)
     with pytest.raises(er.ErError):
         ctx.henry(fw, 298.0, 0, seed=0)
+
+
+def test_henry_device_mask_pipeline(ctx):
+    """grid -> device pocket mask -> Widom with that mask, against the oracle
+    pipeline on the same grid."""
+    import torch
+    f, P, fw = _fw(ctx, 12, n_atoms=424)
+    T = 298.0
+    dims = (40, 40, 40)
+    g = torch.empty(dims, dtype=torch.float32, device="cuda")
+    ctx.grid_device(fw, dims, g.data_ptr())
+    m = torch.empty(dims, dtype=torch.uint8, device="cuda")
+    n_p = ctx.block_pockets_device(g.data_ptr(), dims, T, m.data_ptr())
+    E = g.cpu().numpy().astype(np.float64)
+    ob, on, _ = oracle.block_pockets(E, T)
+    assert n_p == on
+    mask = ((ob == 1e13) & (E != 1e13)).astype(np.uint8)
+    assert np.array_equal(m.cpu().numpy(), mask)
+    n = 50000
+    r = ctx.henry_device_mask(fw, T, n, 21, m.data_ptr(), dims)
+    o = oracle.henry(P, f.t_matrix, f.rep, f.rc2, T, 21, n, mask=mask)
+    assert r["n_blocked"] == o["n_blocked"]
+    kh_o = _kh(o["sum_w"], n, T)
+    assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
