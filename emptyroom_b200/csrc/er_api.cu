@@ -81,8 +81,16 @@ CutoffConsts make_cutoff_consts(double rc2, double /*box_diag*/, double r2min) {
 }
 
 // ------------------------------------------------------------------ kernels
+// Three CTAs per SM (24 warps): the FP32 variants fit 80 registers; the FP64
+// variants (NEAR64, FP64) keep two.
+template <int PREC>
+constexpr int grid_min_blocks() {
+    return (PREC == PREC_NEAR64 || PREC == PREC_FP64) ? 2 : 3;
+}
+
 template <int PREC, int P>
-__global__ void __launch_bounds__(kThreads, 2) grid_kernel(const __grid_constant__ GridTask task) {
+__global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
+    grid_kernel(const __grid_constant__ GridTask task) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
     GridPolicy<P> pol(&task, blockIdx.x);
@@ -92,7 +100,7 @@ __global__ void __launch_bounds__(kThreads, 2) grid_kernel(const __grid_constant
 // One CTA per SM slot pulls (task, brick) items from the queue until it is
 // empty; each task carries its own kernel variant (4 or 8 points per thread).
 template <int PREC>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
     grid_persistent_kernel(const GridTask* __restrict__ tasks, const WorkItem* __restrict__ items,
                            int n_items, int* head) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,6 +141,8 @@ static int configure_variant(er_ctx* ctx) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_NEAR64, P>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_kernel<PREC_FP64, P>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return ER_OK;
 }
 
@@ -163,6 +173,7 @@ int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, floa
     t.nb[1] = (ny + 2 * kWJ - 1) / (2 * kWJ);
     t.nb[2] = (nz + 2 * kWK - 1) / (2 * kWK);
     t.out = out;
+    t.out64 = nullptr;
     return ER_OK;
 }
 
@@ -177,11 +188,13 @@ int launch_grid_plain_on(er_ctx* ctx, const GridTask& t, int prec, cudaStream_t 
         if (prec == PREC_FP32) grid_kernel<PREC_FP32, 8><<<g, kThreads, smem, st>>>(t);
         else if (prec == PREC_COUNT) grid_kernel<PREC_COUNT, 8><<<g, kThreads, smem, st>>>(t);
         else if (prec == PREC_NEAR64) grid_kernel<PREC_NEAR64, 8><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_FP64) grid_kernel<PREC_FP64, 8><<<g, kThreads, smem, st>>>(t);
         else grid_kernel<PREC_COMP, 8><<<g, kThreads, smem, st>>>(t);
     } else {
         if (prec == PREC_FP32) grid_kernel<PREC_FP32, 4><<<g, kThreads, smem, st>>>(t);
         else if (prec == PREC_COUNT) grid_kernel<PREC_COUNT, 4><<<g, kThreads, smem, st>>>(t);
         else if (prec == PREC_NEAR64) grid_kernel<PREC_NEAR64, 4><<<g, kThreads, smem, st>>>(t);
+        else if (prec == PREC_FP64) grid_kernel<PREC_FP64, 4><<<g, kThreads, smem, st>>>(t);
         else grid_kernel<PREC_COMP, 4><<<g, kThreads, smem, st>>>(t);
     }
     ER_CUDA(ctx, cudaGetLastError());
@@ -389,6 +402,7 @@ int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) 
     d.h = hf.h;
     d.inv_h = 1.0 / hf.h;
     for (int k = 0; k < 9; ++k) d.t[k] = hf.t[k];
+    for (int k = 0; k < 9; ++k) d.r[k] = hf.r[k];
     d.rc2 = hf.rc2;
     d.imgs_per_atom = hf.imgs_per_atom;
     rec.bytes = total;
@@ -436,11 +450,34 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
                      : (flags & ER_PREC_FP32)   ? PREC_FP32
                      : (flags & ER_PREC_NEAR64) ? PREC_NEAR64
                                                 : PREC_COMP;
-    if (flags & ER_PREC_FP64)
-        return set_error(ctx, ER_ERR_INVALID, "grid: ER_PREC_FP64 is served by er_grid_fp64");
     const size_t npts = (size_t)nx * ny * nz;
     const bool dev_out = (flags & ER_OUT_DEVICE) != 0;
     const bool f64 = (flags & ER_OUT_F64) != 0;
+    if (flags & ER_PREC_FP64) {
+        // FP64 pair terms and sums, written as FP64
+        if (!f64)
+            return set_error(ctx, ER_ERR_INVALID, "grid: ER_PREC_FP64 needs ER_OUT_F64");
+        if (flags & (ER_COUNT_PAIRS | ER_PREC_FP32 | ER_PREC_NEAR64))
+            return set_error(ctx, ER_ERR_INVALID, "grid: conflicting precision flags");
+        double* d64 = (double*)out;
+        if (!dev_out) {
+            if (ctx->grid_f32.ensure(npts * sizeof(double)) != ER_OK)
+                return set_error(ctx, ER_ERR_NOMEM, "grid: staging allocation failed");
+            d64 = (double*)ctx->grid_f32.ptr;
+        }
+        GridTask t;
+        int st = fill_grid_task(ctx, *f, nx, ny, nz, nullptr, t, tile_p);
+        if (st != ER_OK) return st;
+        t.out64 = d64;
+        st = launch_grid_plain(ctx, t, PREC_FP64);
+        if (st != ER_OK) return st;
+        if (!dev_out) {
+            ER_CUDA(ctx, cudaMemcpyAsync(out, d64, npts * sizeof(double), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+            ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
+        return ER_OK;
+    }
     float* dst = nullptr;
     if (dev_out && !f64) {
         dst = (float*)out;

@@ -5,6 +5,10 @@
 // a + T n, 4 eps s^6 (s^6 - 1) with s = sig^2 / r^2 when r^2 < rc^2.
 // How it computes it is its own:
 //
+//  * Positions live in the framework's positioning frame R (an upper-
+//    triangular rotation of the cell matrix T, equal to T bit for bit when T
+//    is already upper triangular, as the reference's cells are). Distances are
+//    frame-independent; the exact cutoff decision below still uses T.
 //  * A CTA owns up to 8 warp tasks of <= 32*P points (a lattice sub-brick of
 //    the grid, or a chunk of one spatial bin of Widom insertions). The CTA box
 //    is the FP64 bounding box of its points; all FP32 coordinates are relative
@@ -12,18 +16,20 @@
 //  * Candidate atom images come from the framework's cell list: one contiguous
 //    image range per (y, z) row of cells, with the x range of each row pruned
 //    by the cutoff circle. Passing candidates are compacted in order (block
-//    scans, so the order is deterministic) into shared memory as
-//    (dx, dy, dz, C12) + (-C6).
+//    scans, so the order is deterministic) into shared memory.
 //  * Each warp splits the CTA candidates against its own box into an inner
 //    list (inside the cutoff for every point of the warp: no test needed) and
-//    a shell list (cutoff tested per pair). Lists are u16 indices.
-//  * Pair term: u = rcp(r^2) (one MUFU), u3 = u^3, E += u3 (C12 u3 - C6):
-//    10 FP32-pipe instructions per pair on the inner list.
+//    a shell list (cutoff tested per pair). Lists are u16 byte offsets.
+//  * Lattice points of one lane differ only along the grid's first axis, which
+//    R maps to Cartesian x; so per atom the lane forms dy^2 + dz^2 once and per
+//    point only dx and r^2 = dx^2 + (dy^2 + dz^2). Point pairs run as packed
+//    FP32x2 instructions (add/mul/fma .f32x2): per two pair terms 5 packed ops
+//    and 2 MUFU.RCP, E += u^3 (C12 u^3 - C6), u = 1 / r^2.
 //  * Shell pairs whose FP32 r^2 lies within a proven error window of rc^2 are
 //    re-decided in FP64 with the reference's own expression order, so the set
 //    of summed pairs equals the FP64 reference's set exactly.
-//  * Accumulation: FP32 per chunk of 64 atoms, folded into a two-float
-//    (hi, lo) sum with TwoSum (ER_PREC_COMP), or plain FP32 (ER_PREC_FP32).
+//  * Accumulation: FP32 over chunks of 64 atoms, chunks summed in FP64
+//    (ER_PREC_COMP), or FP32 over the whole list (ER_PREC_FP32).
 #pragma once
 #include <float.h>
 #include <math.h>
@@ -38,7 +44,7 @@ constexpr int kThreads = kWarps * 32;
 // points per thread (P) and the CTA brick are set by the point policy (Tile)
 constexpr int kWJ = 4, kWK = 8;            // lanes of a warp sub-brick along j, k
 constexpr int kPMax = 8;                   // largest P any policy uses
-constexpr int kMaxCand = 2048;             // CTA candidate capacity per flush
+constexpr int kMaxCand = 1024;             // CTA candidate capacity per flush
 constexpr int kRowChunk = kThreads;        // cell rows examined per producer pass
 constexpr int kAccChunk = 64;              // atoms per FP32 partial sum
 constexpr float kEnergyCap = 1.0e30f;      // overflow cap (ER_ENERGY_CAP)
@@ -47,42 +53,80 @@ constexpr float kEnergyCap = 1.0e30f;      // overflow cap (ER_ENERGY_CAP)
 // the energy (same traversal; used to count the algorithmic work of a job).
 // PREC_NEAR64 is PREC_COMP with the pairs of atoms within kNearR of a warp's
 // box evaluated in FP64 (they carry most of |E| where terms cancel).
-enum { PREC_COMP = 0, PREC_FP32 = 1, PREC_COUNT = 2, PREC_NEAR64 = 3 };
+// PREC_FP64 evaluates every pair term in FP64 (same pair set).
+enum { PREC_COMP = 0, PREC_FP32 = 1, PREC_COUNT = 2, PREC_NEAR64 = 3, PREC_FP64 = 4 };
 
 template <int PREC>
 struct PrecTraits {
     static constexpr bool comp = PREC == PREC_COMP || PREC == PREC_NEAR64;
     static constexpr bool near64 = PREC == PREC_NEAR64;
+    static constexpr bool fp64 = PREC == PREC_FP64;
 };
 
-constexpr int kNearCap = 256;     // near-list capacity per warp (overflow stays FP32)
+constexpr int kNearCap = 128;     // near-list capacity per warp (overflow stays FP32)
 constexpr float kNearR = 5.0f;    // near radius (A) from the warp box
 
 // One candidate atom image in shared memory (32 bytes, so a list entry can be
-// the byte offset of its record and a load needs no index arithmetic).
+// the byte offset of its record). x, C12 and -C6 are stored twice so that a
+// 128-bit load yields them as packed FP32x2 operands.
 struct __align__(32) Cand {
-    float4 p;    // (dx, dy, dz, C12), position relative to the CTA centre
-    float nc6;   // -C6
-    int id;      // image index (for the FP64 re-decision)
-    float pad0, pad1;
+    float ax, ax_, c12, c12_;    // x, C12 (position relative to the CTA centre)
+    float nc6, nc6_, ay, az;     // -C6, y, z
 };
-
-__device__ __forceinline__ const Cand& cand_at(const Cand* base, unsigned off) {
-    return *reinterpret_cast<const Cand*>(reinterpret_cast<const char*>(base) + off);
-}
 
 struct __align__(16) EngineSmem {
     Cand cand[kMaxCand];                   // CTA candidates
+    int cid[kMaxCand];                     // their image indices (FP64 paths)
     unsigned short wl[kWarps][kMaxCand];   // per-warp inner (front) / shell (back) lists of
                                            // byte offsets into cand
     unsigned short wn[kWarps][kNearCap];   // per-warp near lists (PREC_NEAR64)
+    double tot[kPMax][kThreads];           // FP64 per-point sums, [p][thread]
     int row_beg[kRowChunk];
     int row_off[kRowChunk];
     int warp_tot[kWarps];
     double red[kWarps][6];
-    double box[6];
+    double box[6];                         // CTA box (FP64 lo, hi)
+    float wbox[kWarps][6];                 // warp boxes (local FP32 lo, hi)
     int item;
 };
+
+// ----------------------------------------------------------- packed FP32x2
+typedef unsigned long long f2_t;
+
+__device__ __forceinline__ f2_t f2_pack(float lo, float hi) {
+    f2_t d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void f2_unpack(f2_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2_t f2_sub(f2_t a, f2_t b) {
+    f2_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_add(f2_t a, f2_t b) {
+    f2_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_mul(f2_t a, f2_t b) {
+    f2_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2_t f2_fma(f2_t a, f2_t b, f2_t c) {
+    f2_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// 1.0f when a < b, else 0.0f
+__device__ __forceinline__ float set_lt(float a, float b) {
+    float d;
+    asm("set.lt.f32.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
 
 __device__ __forceinline__ float rcp_approx(float x) {
     float y;
@@ -126,9 +170,10 @@ __device__ __forceinline__ void frac_to_cart(const double* t, double xf, double 
 }
 
 // The reference's FP64 in-cutoff decision for point f and image gid:
-// src/computegridsheet.h:61-79 evaluated in IEEE double without contraction.
+// src/computegridsheet.h:61-79 evaluated in IEEE double without contraction,
+// in the caller's cell matrix T.
 static __device__ __noinline__ bool exact_in_cutoff(const FwDev& fw, const double* f, int gid,
-                                             double r2min) {
+                                                    double r2min) {
     const uint32_t id = fw.img_id[gid];
     const int atom = (int)(id / (uint32_t)fw.imgs_per_atom);
     const int m = (int)(id - (uint32_t)atom * (uint32_t)fw.imgs_per_atom);
@@ -147,33 +192,51 @@ static __device__ __noinline__ bool exact_in_cutoff(const FwDev& fw, const doubl
     return r2 < fw.rc2;
 }
 
-// FP32 pair term with a fixed instruction sequence, so that a later
-// re-evaluation reproduces the same bits.
-__device__ __forceinline__ void pair_r2(float px, float py, float pz, const float4& a,
-                                        float& r2) {
-    const float dx = __fsub_rn(px, a.x);
-    const float dy = __fsub_rn(py, a.y);
-    const float dz = __fsub_rn(pz, a.z);
-    r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-}
-// E_pair = u3 * t with u = 1/r^2, u3 = u^3, t = C12 u3 - C6.
-__device__ __forceinline__ void pair_ut(float r2, float c12, float nc6, float& u3, float& t) {
-    const float u = rcp_approx(r2);
-    u3 = __fmul_rn(__fmul_rn(u, u), u);
-    t = __fmaf_rn(c12, u3, nc6);
+// FP64 pair term of image gid at a point q given relative to the CTA centre o.
+__device__ __forceinline__ double pair64(const FwDev& fw, int gid, double qx, double qy,
+                                         double qz, double o0, double o1, double o2,
+                                         double r2min) {
+    const double4 a = fw.img_xyz[gid];
+    const int atom = (int)(fw.img_id[gid] / (uint32_t)fw.imgs_per_atom);
+    const double2 lj = fw.atom_lj64[atom];
+    const double dx = qx - (a.x - o0), dy = qy - (a.y - o1), dz = qz - (a.z - o2);
+    double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+    r2 = fmax(r2, r2min);
+    const double u = __drcp_rn(r2);
+    const double u3 = u * u * u;
+    return u3 * fma(lj.x, u3, -lj.y);
 }
 
-__device__ __forceinline__ void two_sum_into(float& hi, float& lo, float a) {
-    const float s = __fadd_rn(hi, a);
-    const float bp = __fsub_rn(s, hi);
-    const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(a, bp));
-    hi = s;
-    lo = __fadd_rn(lo, e);
+// FP32 r^2 of the generic form (each point has its own x, y, z) and of the
+// lattice form (ss = dy^2 + dz^2 shared by a lane's points). Both are fixed
+// instruction sequences, so a later re-evaluation reproduces the same bits.
+__device__ __forceinline__ float r2_generic(float px, float py, float pz, float ax, float ay,
+                                            float az) {
+    const float dx = __fsub_rn(px, ax);
+    const float dy = __fsub_rn(py, ay);
+    const float dz = __fsub_rn(pz, az);
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+__device__ __forceinline__ float ss_lattice(float py, float pz, float ay, float az) {
+    const float dy = __fsub_rn(py, ay);
+    const float dz = __fsub_rn(pz, az);
+    return __fmaf_rn(dz, dz, __fmul_rn(dy, dy));
+}
+__device__ __forceinline__ float r2_lattice(float px, float ax, float ss) {
+    const float dx = __fsub_rn(px, ax);
+    return __fmaf_rn(dx, dx, ss);
+}
+// E_pair = u3 * t with u = 1/r^2, u3 = u^3, t = C12 u3 - C6.
+__device__ __forceinline__ float pair_term(float r2, float c12, float nc6) {
+    const float u = rcp_approx(r2);
+    const float u3 = __fmul_rn(__fmul_rn(u, u), u);
+    return __fmul_rn(u3, __fmaf_rn(c12, u3, nc6));
 }
 
 // ---------------------------------------------------------------------------
 // Point sources. A policy maps (warp, lane, p) to an FP64 fractional point
-// and stores its energy.
+// and stores its energy. kLattice: a lane's P points differ only in the
+// first fractional coordinate.
 
 // Lattice points of one (2P) x 8 x 16 brick of a grid job: warp w owns the
 // P x 4 x 8 sub-brick at ((w & 1) P, ((w >> 1) & 1) 4, (w >> 2) 8); lane l the
@@ -181,6 +244,7 @@ __device__ __forceinline__ void two_sum_into(float& hi, float& lo, float a) {
 template <int P_>
 struct GridPolicy {
     static constexpr int kP = P_;
+    static constexpr bool kLattice = true;
     static constexpr int kBI = 2 * P_, kBJ = 2 * kWJ, kBK = 2 * kWK;
     const GridTask* T;
     int i0, j0, k0;
@@ -196,6 +260,8 @@ struct GridPolicy {
         j = j0 + ((w >> 1) & 1) * kWJ + lane / kWK;
         k = k0 + (w >> 2) * kWK + lane % kWK;
     }
+    // Out-of-range points are clamped onto the lattice (same j, k when only i
+    // overshoots, so a lane's points keep sharing y and z) and never stored.
     __device__ __forceinline__ bool point(int w, int lane, int p, double* f) const {
         int i, j, k;
         index(w, lane, p, i, j, k);
@@ -213,6 +279,12 @@ struct GridPolicy {
         if (i < T->nx && j < T->ny && k < T->nz)
             T->out[(size_t)k + (size_t)j * T->nz + (size_t)i * T->ny * T->nz] = e;
     }
+    __device__ __forceinline__ void store64(int w, int lane, int p, double e) const {
+        int i, j, k;
+        index(w, lane, p, i, j, k);
+        if (i < T->nx && j < T->ny && k < T->nz)
+            T->out64[(size_t)k + (size_t)j * T->nz + (size_t)i * T->ny * T->nz] = e;
+    }
 };
 
 // Widom insertion points: CTA c owns sorted positions [256 P c, 256 P (c + 1))
@@ -220,6 +292,7 @@ struct GridPolicy {
 template <int P_>
 struct PointPolicy {
     static constexpr int kP = P_;
+    static constexpr bool kLattice = false;
     const PointTask* T;
     int base, nv;
     __device__ PointPolicy(const PointTask* task, int cta)
@@ -240,6 +313,9 @@ struct PointPolicy {
     __device__ __forceinline__ void store(int w, int lane, int p, float e) const {
         const int idx = slot_index(w, lane, p);
         if (idx >= 0) T->energies[idx] = e;
+    }
+    __device__ __forceinline__ void store64(int w, int lane, int p, double e) const {
+        store(w, lane, p, (float)e);
     }
 };
 
@@ -262,36 +338,304 @@ __device__ __forceinline__ int borderline_ulps(double rc, float rc2f, double box
     return 2 * ((int)ceil(err / ulpR) + 2);
 }
 
+// Per-thread state of one CTA pass. The FP64 per-point sums live in shared
+// memory (EngineSmem::tot), the warp box and the CTA centre too.
+template <class Pol, int PREC>
+struct Lane {
+    static constexpr int P = Pol::kP;
+    static constexpr int NY = Pol::kLattice ? 1 : P;  // distinct y, z per lane
+    float px[P], py[NY], pz[NY];
+    unsigned vmask;
+    bool warp_live;
+    int bul;
+};
+
+__device__ __forceinline__ double& tot_at(EngineSmem& s, int p) {
+    return s.tot[p][threadIdx.x];
+}
+
+// Folds FP32 chunk sums into the FP64 totals.
+template <int M>
+__device__ __forceinline__ void fold_packed(EngineSmem& s, f2_t* acc2) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float a0, a1;
+        f2_unpack(acc2[m], a0, a1);
+        tot_at(s, 2 * m) += (double)a0;
+        tot_at(s, 2 * m + 1) += (double)a1;
+        acc2[m] = 0ull;
+    }
+}
+
+__device__ __forceinline__ void cta_centre(const EngineSmem& s, double& o0, double& o1,
+                                           double& o2) {
+    o0 = 0.5 * (s.box[0] + s.box[3]);
+    o1 = 0.5 * (s.box[1] + s.box[4]);
+    o2 = 0.5 * (s.box[2] + s.box[5]);
+}
+
+// Lattice inner list: every pair inside the cutoff, packed over point pairs.
+template <class Pol, int PREC>
+__device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned short* wl,
+                                              int n_in, Lane<Pol, PREC>& L) {
+    constexpr int M = Pol::kP / 2;
+    constexpr bool kComp = PrecTraits<PREC>::comp;
+    f2_t px2[M], acc2[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        px2[m] = f2_pack(L.px[2 * m], L.px[2 * m + 1]);
+        acc2[m] = 0ull;
+    }
+    const f2_t one2 = f2_pack(1.0f, 1.0f);
+    const float py = L.py[0], pz = L.pz[0];
+    const char* cbase = reinterpret_cast<const char*>(s.cand);
+    const unsigned* wl32 = reinterpret_cast<const unsigned*>(wl);
+    auto atom = [&](unsigned off) {
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
+        const float4 v1 = *reinterpret_cast<const float4*>(cbase + off + 16);
+        if (PREC == PREC_COUNT) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) acc2[m] = f2_add(acc2[m], one2);
+            return;
+        }
+        const f2_t nc6 = f2_pack(v1.x, v1.y);
+        const float ss = ss_lattice(py, pz, v1.z, v1.w);
+        const f2_t ss2 = f2_pack(ss, ss);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const f2_t dx = f2_sub(px2[m], v0.x);
+            const f2_t r2 = f2_fma(dx, dx, ss2);
+            float r0, r1;
+            f2_unpack(r2, r0, r1);
+            const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
+            const f2_t u3 = f2_mul(f2_mul(u, u), u);
+            acc2[m] = f2_fma(u3, f2_fma(v0.y, u3, nc6), acc2[m]);
+        }
+    };
+    int q = 0;
+    while (q < n_in) {
+        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
+        for (; q + 1 < qe; q += 2) {  // q is even here: chunks are 64 entries
+            const unsigned two = wl32[q >> 1];
+            atom(two & 0xffffu);
+            atom(two >> 16);
+        }
+        if (q < qe) atom(wl[q++]);
+        if (kComp) fold_packed<M>(s, acc2);
+    }
+    if (!kComp) fold_packed<M>(s, acc2);
+}
+
+// Lattice shell list: cutoff tested per pair (mask 1.0 / 0.0), and the
+// smallest |r^2 - fl32(rc^2)| per point pair kept for the borderline test.
+template <class Pol, int PREC>
+__device__ __forceinline__ void lattice_shell(EngineSmem& s, const unsigned short* wl,
+                                              int n_sh, float rc2f, Lane<Pol, PREC>& L,
+                                              float* mnd) {
+    constexpr int M = Pol::kP / 2;
+    constexpr bool kComp = PrecTraits<PREC>::comp;
+    f2_t px2[M], acc2[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        px2[m] = f2_pack(L.px[2 * m], L.px[2 * m + 1]);
+        acc2[m] = 0ull;
+        mnd[m] = INFINITY;
+    }
+    const f2_t rc2 = f2_pack(rc2f, rc2f);
+    const float py = L.py[0], pz = L.pz[0];
+    const char* cbase = reinterpret_cast<const char*>(s.cand);
+    // the shell list runs backwards from the end of wl
+    const unsigned* wl32 = reinterpret_cast<const unsigned*>(wl);
+    auto atom = [&](unsigned off) {
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
+        const float4 v1 = *reinterpret_cast<const float4*>(cbase + off + 16);
+        const f2_t nc6 = f2_pack(v1.x, v1.y);
+        const float ss = ss_lattice(py, pz, v1.z, v1.w);
+        const f2_t ss2 = f2_pack(ss, ss);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const f2_t dx = f2_sub(px2[m], v0.x);
+            const f2_t r2 = f2_fma(dx, dx, ss2);
+            float r0, r1, d0, d1;
+            f2_unpack(r2, r0, r1);
+            const f2_t in = f2_pack(set_lt(r0, rc2f), set_lt(r1, rc2f));
+            f2_unpack(f2_sub(r2, rc2), d0, d1);
+            mnd[m] = fminf(mnd[m], fminf(fabsf(d0), fabsf(d1)));
+            if (PREC == PREC_COUNT) {
+                acc2[m] = f2_add(acc2[m], in);
+            } else {
+                const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
+                const f2_t u3 = f2_mul(f2_mul(u, u), u);
+                acc2[m] = f2_fma(f2_mul(u3, in), f2_fma(v0.y, u3, nc6), acc2[m]);
+            }
+        }
+    };
+    int q = 0;
+    while (q < n_sh) {
+        const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
+        for (; q + 1 < qe; q += 2) {
+            // entries q, q+1 sit at wl[K-1-q], wl[K-2-q]: one aligned u32
+            const unsigned two = wl32[(kMaxCand - 2 - q) >> 1];
+            atom(two >> 16);
+            atom(two & 0xffffu);
+        }
+        if (q < qe) {
+            atom(wl[kMaxCand - 1 - q]);
+            ++q;
+        }
+        if (kComp) fold_packed<M>(s, acc2);
+    }
+    if (!kComp) fold_packed<M>(s, acc2);
+}
+
+// Generic (per-point x, y, z) inner and shell lists, scalar FP32.
+template <class Pol, int PREC>
+__device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned short* wl,
+                                              int n_in, int n_sh, float rc2f, float win,
+                                              Lane<Pol, PREC>& L, unsigned& bflag) {
+    constexpr int P = Pol::kP;
+    constexpr bool kComp = PrecTraits<PREC>::comp;
+    float acc[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) acc[p] = 0.f;
+    int q = 0;
+    while (q < n_in) {
+        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
+#pragma unroll 2
+        for (; q < qe; ++q) {
+            const Cand& cd = *reinterpret_cast<const Cand*>(
+                reinterpret_cast<const char*>(s.cand) + wl[q]);
+            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);
+            const float4 v1 = *reinterpret_cast<const float4*>(&cd.nc6);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                if (PREC == PREC_COUNT) {
+                    acc[p] += 1.0f;
+                } else {
+                    const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v1.z, v1.w);
+                    const float u = rcp_approx(r2);
+                    const float u3 = __fmul_rn(__fmul_rn(u, u), u);
+                    acc[p] = __fmaf_rn(u3, __fmaf_rn(v0.z, u3, v1.x), acc[p]);
+                }
+            }
+        }
+        if (kComp) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                tot_at(s, p) += (double)acc[p];
+                acc[p] = 0.f;
+            }
+        }
+    }
+    bool bf[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) bf[p] = false;
+    q = 0;
+    while (q < n_sh) {
+        const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
+#pragma unroll 2
+        for (; q < qe; ++q) {
+            const Cand& cd = *reinterpret_cast<const Cand*>(
+                reinterpret_cast<const char*>(s.cand) + wl[kMaxCand - 1 - q]);
+            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);
+            const float4 v1 = *reinterpret_cast<const float4*>(&cd.nc6);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v1.z, v1.w);
+                const float dd = __fsub_rn(r2, rc2f);
+                if (PREC == PREC_COUNT) {
+                    if (dd < 0.f) acc[p] += 1.0f;
+                } else {
+                    const float u = rcp_approx(r2);
+                    const float u3 = __fmul_rn(__fmul_rn(u, u), u);
+                    if (dd < 0.f) acc[p] = __fmaf_rn(u3, __fmaf_rn(v0.z, u3, v1.x), acc[p]);
+                }
+                bf[p] = bf[p] || (fabsf(dd) <= win);
+            }
+        }
+        if (kComp) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                tot_at(s, p) += (double)acc[p];
+                acc[p] = 0.f;
+            }
+        }
+    }
+    if (!kComp) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) tot_at(s, p) += (double)acc[p];
+    }
+    bflag = 0;
+#pragma unroll
+    for (int p = 0; p < P; ++p) bflag |= bf[p] ? (1u << p) : 0u;
+}
+
+// Exact re-decision of the borderline shell pairs of the points flagged in
+// bflag: a pair whose FP32 r^2 is within `win` of fl32(rc^2) is decided by
+// exact_in_cutoff, and its term added or removed where the FP32 decision
+// differed. Kept out of line: it runs for a few lanes of a few warps.
+template <class Pol, int PREC>
+static __device__ __noinline__ void recheck_borderline(EngineSmem& s, const Pol& pol,
+                                                       const FwDev& fw, const CutoffConsts& cc,
+                                                       const unsigned short* wl, int n_sh,
+                                                       float win, unsigned bflag,
+                                                       const Lane<Pol, PREC>& L) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const float rc2f = cc.rc2f;
+    for (int qq = 0; qq < n_sh; ++qq) {
+        const unsigned off = wl[kMaxCand - 1 - qq];
+        const Cand& cd = s.cand[off >> 5];
+        const float ss = Pol::kLattice ? ss_lattice(L.py[0], L.pz[0], cd.ay, cd.az) : 0.f;
+#pragma unroll 1
+        for (int p = 0; p < Pol::kP; ++p) {
+            if (!(bflag & (1u << p))) continue;
+            const float r2 =
+                Pol::kLattice ? r2_lattice(L.px[p], cd.ax, ss)
+                              : r2_generic(L.px[p], L.py[Pol::kLattice ? 0 : p],
+                                           L.pz[Pol::kLattice ? 0 : p], cd.ax, cd.ay, cd.az);
+            const float dd = __fsub_rn(r2, rc2f);
+            if (fabsf(dd) <= win) {
+                double f[3];
+                pol.point(w, lane, p, f);
+                const bool ex = exact_in_cutoff(fw, f, s.cid[off >> 5], cc.r2min);
+                if (ex != (dd < 0.f)) {
+                    const float e = PREC == PREC_COUNT ? 1.0f : pair_term(r2, cd.c12, cd.nc6);
+                    tot_at(s, p) += ex ? (double)e : -(double)e;
+                }
+            }
+        }
+    }
+}
+
 template <class Pol, int PREC>
 __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
                                            const CutoffConsts& cc, int n_cand,
-                                           const float* px, const float* py, const float* pz,
-                                           float* hi, float* lo, double* nacc, float wl0x,
-                                           float wl0y, float wl0z, float wh0x, float wh0y,
-                                           float wh0z, bool warp_live, unsigned vmask,
-                                           int bul_i) {
-    constexpr bool kComp = PrecTraits<PREC>::comp;
+                                           Lane<Pol, PREC>& L) {
+    constexpr int P = Pol::kP;
     constexpr bool kNear = PrecTraits<PREC>::near64;
+    constexpr bool kF64 = PrecTraits<PREC>::fp64;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (!warp_live) return;
+    if (!L.warp_live) return;
     unsigned short* wl = s.wl[w];
     unsigned short* wn = s.wn[w];
     // --- split candidates into inner / shell (/ near) lists for this warp's box
     int n_in = 0, n_sh = 0, n_near = 0;
     const unsigned lt = (1u << lane) - 1u;
     const float rnear2 = kNearR * kNearR;
+    const float wl0x = s.wbox[w][0], wl0y = s.wbox[w][1], wl0z = s.wbox[w][2];
+    const float wh0x = s.wbox[w][3], wh0y = s.wbox[w][4], wh0z = s.wbox[w][5];
     for (int base = 0; base < n_cand; base += 32) {
         const int c = base + lane;
         bool in = false, sh = false, nr = false;
         if (c < n_cand) {
-            const float4 a = s.cand[c].p;
-            const float ex = fmaxf(0.f, fmaxf(wl0x - a.x, a.x - wh0x));
-            const float ey = fmaxf(0.f, fmaxf(wl0y - a.y, a.y - wh0y));
-            const float ez = fmaxf(0.f, fmaxf(wl0z - a.z, a.z - wh0z));
+            const float ax = s.cand[c].ax, ay = s.cand[c].ay, az = s.cand[c].az;
+            const float ex = fmaxf(0.f, fmaxf(wl0x - ax, ax - wh0x));
+            const float ey = fmaxf(0.f, fmaxf(wl0y - ay, ay - wh0y));
+            const float ez = fmaxf(0.f, fmaxf(wl0z - az, az - wh0z));
             const float dmin2 = ex * ex + ey * ey + ez * ez;
-            const float fx = fmaxf(fabsf(a.x - wl0x), fabsf(a.x - wh0x));
-            const float fy = fmaxf(fabsf(a.y - wl0y), fabsf(a.y - wh0y));
-            const float fz = fmaxf(fabsf(a.z - wl0z), fabsf(a.z - wh0z));
+            const float fx = fmaxf(fabsf(ax - wl0x), fabsf(ax - wh0x));
+            const float fy = fmaxf(fabsf(ay - wl0y), fabsf(ay - wh0y));
+            const float fz = fmaxf(fabsf(az - wl0z), fabsf(az - wh0z));
             const float dmax2 = fx * fx + fy * fy + fz * fz;
             in = dmax2 < cc.rin2;
             sh = !in && dmin2 < cc.rout2;
@@ -317,173 +661,115 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
     }
     __syncwarp();
 
-    // --- inner list: every pair is inside the cutoff
-    float acc[Pol::kP];
-#pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) acc[p] = 0.f;
-    int q = 0;
-    while (q < n_in) {
-        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
-#pragma unroll 2
-        for (; q < qe; ++q) {
-            const Cand& cd = cand_at(s.cand, wl[q]);
-            const float4 a = cd.p;
-            const float nc6 = cd.nc6;
-#pragma unroll
-            for (int p = 0; p < Pol::kP; ++p) {
-                if (PREC == PREC_COUNT) {
-                    acc[p] += 1.0f;
-                } else {
-                    float r2, u3, t;
-                    pair_r2(px[p], py[p], pz[p], a, r2);
-                    pair_ut(r2, a.w, nc6, u3, t);
-                    acc[p] = __fmaf_rn(u3, t, acc[p]);
-                }
-            }
-        }
-        if (kComp) {
-#pragma unroll
-            for (int p = 0; p < Pol::kP; ++p) {
-                two_sum_into(hi[p], lo[p], acc[p]);
-                acc[p] = 0.f;
-            }
-        }
-    }
-    // --- shell list: cutoff tested per pair, borderline pairs flagged.
-    // dd = r^2 - fl32(rc^2) is exact wherever |dd| is near the window
-    // (Sterbenz), so |dd| <= win selects exactly the pairs within bul ulps.
     const float rc2f = cc.rc2f;
     float win;
     {
         int e;
         frexpf(rc2f, &e);
-        win = ldexpf((float)bul_i, e - 24);
+        win = ldexpf((float)L.bul, e - 24);
     }
-    bool bf[Pol::kP];
-#pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) bf[p] = false;
-    q = 0;
-    while (q < n_sh) {
-        const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
-#pragma unroll 2
-        for (; q < qe; ++q) {
-            const Cand& cd = cand_at(s.cand, wl[kMaxCand - 1 - q]);
-            const float4 a = cd.p;
-            const float nc6 = cd.nc6;
-#pragma unroll
-            for (int p = 0; p < Pol::kP; ++p) {
-                float r2, u3, t;
-                pair_r2(px[p], py[p], pz[p], a, r2);
-                const float dd = __fsub_rn(r2, rc2f);
-                if (PREC == PREC_COUNT) {
-                    if (dd < 0.f) acc[p] += 1.0f;
-                } else {
-                    pair_ut(r2, a.w, nc6, u3, t);
-                    if (dd < 0.f) acc[p] = __fmaf_rn(u3, t, acc[p]);
-                }
-                bf[p] = bf[p] || (fabsf(dd) <= win);
-            }
-        }
-        if (kComp) {
-#pragma unroll
-            for (int p = 0; p < Pol::kP; ++p) {
-                two_sum_into(hi[p], lo[p], acc[p]);
-                acc[p] = 0.f;
-            }
-        }
-    }
-    if (!kComp) {
-#pragma unroll
-        for (int p = 0; p < Pol::kP; ++p) hi[p] = __fadd_rn(hi[p], acc[p]);
-    }
-    // --- exact re-decision of borderline shell pairs (rare)
+
+    // FP64 positions of this lane's points relative to the CTA centre
+    // (FP64 paths only).
+    auto point64 = [&](int p, double& qx, double& qy, double& qz) {
+        double f[3], x, y, z, o0, o1, o2;
+        pol.point(w, lane, p, f);
+        frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
+        cta_centre(s, o0, o1, o2);
+        qx = x - o0;
+        qy = y - o1;
+        qz = z - o2;
+    };
+
     unsigned bflag = 0;
-#pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) bflag |= bf[p] ? (1u << p) : 0u;
-    bflag &= vmask;
-    if (__any_sync(0xffffffffu, bflag != 0)) {
-        for (int p = 0; p < Pol::kP; ++p) {
-            if (!(bflag & (1u << p))) continue;
+    if (kF64) {
+        // every inner pair in FP64; shell pairs decided as below, term in FP64
+        double o0, o1, o2;
+        cta_centre(s, o0, o1, o2);
+#pragma unroll 1
+        for (int p = 0; p < P; ++p) {
+            double qx, qy, qz;
+            point64(p, qx, qy, qz);
+            double acc = 0.0;
+            for (int q = 0; q < n_in; ++q)
+                acc += pair64(fw, s.cid[wl[q] >> 5], qx, qy, qz, o0, o1, o2, cc.r2min);
             double f[3];
             pol.point(w, lane, p, f);
-            float corr = 0.f;
-            for (int qq = 0; qq < n_sh; ++qq) {
-                const Cand& cd = cand_at(s.cand, wl[kMaxCand - 1 - qq]);
-                const float4 a = cd.p;
-                float r2;
-                pair_r2(px[p], py[p], pz[p], a, r2);
+            for (int q = 0; q < n_sh; ++q) {
+                const unsigned off = wl[kMaxCand - 1 - q];
+                const Cand& cd = s.cand[off >> 5];
+                const float r2 = Pol::kLattice
+                                     ? r2_lattice(L.px[p], cd.ax, ss_lattice(L.py[0], L.pz[0],
+                                                                             cd.ay, cd.az))
+                                     : r2_generic(L.px[p], L.py[Pol::kLattice ? 0 : p],
+                                                  L.pz[Pol::kLattice ? 0 : p], cd.ax, cd.ay,
+                                                  cd.az);
                 const float dd = __fsub_rn(r2, rc2f);
-                if (fabsf(dd) <= win) {
-                    const bool ex = exact_in_cutoff(fw, f, cd.id, cc.r2min);
-                    if (ex != (dd < 0.f)) {
-                        float e = 1.0f;
-                        if (PREC != PREC_COUNT) {
-                            float u3, t;
-                            pair_ut(r2, a.w, cd.nc6, u3, t);
-                            e = __fmul_rn(u3, t);
-                        }
-                        corr = ex ? __fadd_rn(corr, e) : __fsub_rn(corr, e);
-                    }
-                }
+                bool inside = dd < 0.f;
+                if (fabsf(dd) <= win) inside = exact_in_cutoff(fw, f, s.cid[off >> 5], cc.r2min);
+                if (inside)
+                    acc += pair64(fw, s.cid[off >> 5], qx, qy, qz, o0, o1, o2, cc.r2min);
             }
-            if (kComp) two_sum_into(hi[p], lo[p], corr);
-            else hi[p] = __fadd_rn(hi[p], corr);
+            tot_at(s, p) += acc;
         }
+        return;
     }
+
+    if (Pol::kLattice) {
+        float mnd[P / 2];
+        lattice_inner<Pol, PREC>(s, wl, n_in, L);
+        lattice_shell<Pol, PREC>(s, wl, n_sh, rc2f, L, mnd);
+#pragma unroll
+        for (int m = 0; m < P / 2; ++m) bflag |= (mnd[m] <= win) ? (3u << (2 * m)) : 0u;
+    } else {
+        generic_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, bflag);
+    }
+
+    // --- exact re-decision of borderline shell pairs (rare); lanes without a
+    // flagged point idle through it
+    bflag &= L.vmask;
+    if (bflag) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, bflag, L);
     // --- near list in FP64: exact positions (FP64 images and points relative
     // to the CTA centre) and FP64 (C12, C6); all near atoms are inner atoms.
     if (kNear && n_near > 0) {
-        const double o0 = 0.5 * (s.box[0] + s.box[3]);
-        const double o1 = 0.5 * (s.box[1] + s.box[4]);
-        const double o2 = 0.5 * (s.box[2] + s.box[5]);
-        double qx[Pol::kP], qy[Pol::kP], qz[Pol::kP];
+        double qx[P], qy[P], qz[P], o0, o1, o2;
+        cta_centre(s, o0, o1, o2);
 #pragma unroll
-        for (int p = 0; p < Pol::kP; ++p) {
-            double f[3], x, y, z;
-            pol.point(w, lane, p, f);
-            frac_to_cart(fw.t, f[0], f[1], f[2], x, y, z);
-            qx[p] = x - o0;
-            qy[p] = y - o1;
-            qz[p] = z - o2;
-        }
+        for (int p = 0; p < P; ++p) point64(p, qx[p], qy[p], qz[p]);
+        double nacc[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) nacc[p] = 0.0;
         for (int q = 0; q < n_near; ++q) {
-            const Cand& cd = cand_at(s.cand, wn[q]);
-            const double4 a = fw.img_xyz[cd.id];
-            const int atom = (int)(fw.img_id[cd.id] / (uint32_t)fw.imgs_per_atom);
-            const double2 lj = fw.atom_lj64[atom];
-            const double ax = a.x - o0, ay = a.y - o1, az = a.z - o2;
+            const int gid = s.cid[wn[q] >> 5];
 #pragma unroll
-            for (int p = 0; p < Pol::kP; ++p) {
-                const double dx = qx[p] - ax, dy = qy[p] - ay, dz = qz[p] - az;
-                double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
-                r2 = fmax(r2, cc.r2min);
-                const double u = __drcp_rn(r2);
-                const double u3 = u * u * u;
-                nacc[p] = fma(u3, fma(lj.x, u3, -lj.y), nacc[p]);
-            }
+            for (int p = 0; p < P; ++p)
+                nacc[p] += pair64(fw, gid, qx[p], qy[p], qz[p], o0, o1, o2, cc.r2min);
         }
+#pragma unroll
+        for (int p = 0; p < P; ++p) tot_at(s, p) += nacc[p];
     }
 }
 
 template <class Pol, int PREC>
 __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                             const CutoffConsts& cc) {
+    constexpr int P = Pol::kP;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    Lane<Pol, PREC> L;
 
-    // 1. FP64 Cartesian points and the CTA box.
-    double cx[Pol::kP], cy[Pol::kP], cz[Pol::kP];
-    unsigned vmask = 0;
+    // 1. the CTA box: FP64 bounding box of the valid points
+    L.vmask = 0;
     double mn0 = INFINITY, mn1 = INFINITY, mn2 = INFINITY;
     double mx0 = -INFINITY, mx1 = -INFINITY, mx2 = -INFINITY;
 #pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) {
-        double f[3];
+    for (int p = 0; p < P; ++p) {
+        double f[3], x, y, z;
         const bool ok = pol.point(w, lane, p, f);
-        frac_to_cart(fw.t, f[0], f[1], f[2], cx[p], cy[p], cz[p]);
+        frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
         if (ok) {
-            vmask |= 1u << p;
-            mn0 = fmin(mn0, cx[p]); mn1 = fmin(mn1, cy[p]); mn2 = fmin(mn2, cz[p]);
-            mx0 = fmax(mx0, cx[p]); mx1 = fmax(mx1, cy[p]); mx2 = fmax(mx2, cz[p]);
+            L.vmask |= 1u << p;
+            mn0 = fmin(mn0, x); mn1 = fmin(mn1, y); mn2 = fmin(mn2, z);
+            mx0 = fmax(mx0, x); mx1 = fmax(mx1, y); mx2 = fmax(mx2, z);
         }
     }
 #pragma unroll
@@ -495,7 +781,7 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
         mx1 = fmax(mx1, __shfl_xor_sync(0xffffffffu, mx1, o));
         mx2 = fmax(mx2, __shfl_xor_sync(0xffffffffu, mx2, o));
     }
-    const bool warp_live = __any_sync(0xffffffffu, vmask != 0);
+    L.warp_live = __any_sync(0xffffffffu, L.vmask != 0);
     if (lane == 0) {
         s.red[w][0] = mn0; s.red[w][1] = mn1; s.red[w][2] = mn2;
         s.red[w][3] = mx0; s.red[w][4] = mx1; s.red[w][5] = mx2;
@@ -512,37 +798,48 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     const double hi0 = s.box[3], hi1 = s.box[4], hi2 = s.box[5];
     __syncthreads();
     if (!(lo0 <= hi0)) return;  // no valid point in this CTA
-    const double o0 = 0.5 * (lo0 + hi0), o1 = 0.5 * (lo1 + hi1), o2 = 0.5 * (lo2 + hi2);
-    const int bul = borderline_ulps(
+    double o0, o1, o2;
+    cta_centre(s, o0, o1, o2);
+    L.bul = borderline_ulps(
         cc.rc, cc.rc2f,
         sqrt((hi0 - lo0) * (hi0 - lo0) + (hi1 - lo1) * (hi1 - lo1) + (hi2 - lo2) * (hi2 - lo2)));
 
-    // 2. local FP32 coordinates and the warp box
-    float px[Pol::kP], py[Pol::kP], pz[Pol::kP], hi[Pol::kP], lo[Pol::kP];
-    double nacc[PrecTraits<PREC>::near64 ? Pol::kP : 1];
+    // 2. local FP32 coordinates and the warp box (a lattice lane's points
+    // share y and z bit for bit: R[1][0] = R[2][0] = 0)
+    {
+        float wl0x = INFINITY, wl0y = INFINITY, wl0z = INFINITY;
+        float wh0x = -INFINITY, wh0y = -INFINITY, wh0z = -INFINITY;
 #pragma unroll
-    for (int p = 0; p < (PrecTraits<PREC>::near64 ? Pol::kP : 1); ++p) nacc[p] = 0.0;
-    float wl0x = INFINITY, wl0y = INFINITY, wl0z = INFINITY;
-    float wh0x = -INFINITY, wh0y = -INFINITY, wh0z = -INFINITY;
-#pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) {
-        px[p] = (float)(cx[p] - o0);
-        py[p] = (float)(cy[p] - o1);
-        pz[p] = (float)(cz[p] - o2);
-        hi[p] = 0.f; lo[p] = 0.f;
-        if (vmask & (1u << p)) {
-            wl0x = fminf(wl0x, px[p]); wl0y = fminf(wl0y, py[p]); wl0z = fminf(wl0z, pz[p]);
-            wh0x = fmaxf(wh0x, px[p]); wh0y = fmaxf(wh0y, py[p]); wh0z = fmaxf(wh0z, pz[p]);
+        for (int p = 0; p < P; ++p) {
+            double f[3], x, y, z;
+            pol.point(w, lane, p, f);
+            frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
+            const float fx = (float)(x - o0), fy = (float)(y - o1), fz = (float)(z - o2);
+            L.px[p] = fx;
+            if (!Pol::kLattice || p == 0) {
+                L.py[Pol::kLattice ? 0 : p] = fy;
+                L.pz[Pol::kLattice ? 0 : p] = fz;
+            }
+            tot_at(s, p) = 0.0;
+            if (L.vmask & (1u << p)) {
+                wl0x = fminf(wl0x, fx); wl0y = fminf(wl0y, fy); wl0z = fminf(wl0z, fz);
+                wh0x = fmaxf(wh0x, fx); wh0y = fmaxf(wh0y, fy); wh0z = fmaxf(wh0z, fz);
+            }
         }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        wl0x = fminf(wl0x, __shfl_xor_sync(0xffffffffu, wl0x, o));
-        wl0y = fminf(wl0y, __shfl_xor_sync(0xffffffffu, wl0y, o));
-        wl0z = fminf(wl0z, __shfl_xor_sync(0xffffffffu, wl0z, o));
-        wh0x = fmaxf(wh0x, __shfl_xor_sync(0xffffffffu, wh0x, o));
-        wh0y = fmaxf(wh0y, __shfl_xor_sync(0xffffffffu, wh0y, o));
-        wh0z = fmaxf(wh0z, __shfl_xor_sync(0xffffffffu, wh0z, o));
+        for (int o = 16; o > 0; o >>= 1) {
+            wl0x = fminf(wl0x, __shfl_xor_sync(0xffffffffu, wl0x, o));
+            wl0y = fminf(wl0y, __shfl_xor_sync(0xffffffffu, wl0y, o));
+            wl0z = fminf(wl0z, __shfl_xor_sync(0xffffffffu, wl0z, o));
+            wh0x = fmaxf(wh0x, __shfl_xor_sync(0xffffffffu, wh0x, o));
+            wh0y = fmaxf(wh0y, __shfl_xor_sync(0xffffffffu, wh0y, o));
+            wh0z = fmaxf(wh0z, __shfl_xor_sync(0xffffffffu, wh0z, o));
+        }
+        if (lane == 0) {
+            s.wbox[w][0] = wl0x; s.wbox[w][1] = wl0y; s.wbox[w][2] = wl0z;
+            s.wbox[w][3] = wh0x; s.wbox[w][4] = wh0y; s.wbox[w][5] = wh0z;
+        }
+        __syncwarp();
     }
 
     // 3. producer: rows of cells around the CTA box, streamed into shared memory
@@ -593,8 +890,7 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
             for (int cb = 0; cb < tot; cb += kThreads) {
                 const int c = cb + tid;
                 int pass = 0, g = 0;
-                float4 cp = make_float4(0.f, 0.f, 0.f, 0.f);
-                float nc6 = 0.f;
+                float ax = 0.f, ay = 0.f, az = 0.f, c12 = 0.f, nc6 = 0.f;
                 if (c < tot) {
                     int a = 0, b = nr - 1;
                     while (a < b) {
@@ -603,15 +899,16 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                     }
                     g = s.row_beg[a] + (c - s.row_off[a]);
                     const double4 ap = fw.img_xyz[g];
-                    const float ax = (float)(ap.x - o0), ay = (float)(ap.y - o1),
-                                az = (float)(ap.z - o2);
+                    ax = (float)(ap.x - o0);
+                    ay = (float)(ap.y - o1);
+                    az = (float)(ap.z - o2);
                     const float ddx = fmaxf(0.f, fmaxf(b0x - ax, ax - b1x));
                     const float ddy = fmaxf(0.f, fmaxf(b0y - ay, ay - b1y));
                     const float ddz = fmaxf(0.f, fmaxf(b0z - az, az - b1z));
                     pass = (ddx * ddx + ddy * ddy + ddz * ddz) < R2f;
                     if (pass) {
                         const float2 pr = fw.img_par[g];
-                        cp = make_float4(ax, ay, az, pr.x);
+                        c12 = pr.x;
                         nc6 = pr.y;
                     }
                 }
@@ -619,16 +916,15 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                 const int pos = block_exscan(pass, s.warp_tot, &npass);
                 if (n_cand + npass > kMaxCand) {
                     __syncthreads();
-                    warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, nacc, wl0x,
-                                          wl0y, wl0z, wh0x, wh0y, wh0z, warp_live, vmask, bul);
+                    warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, L);
                     __syncthreads();
                     n_cand = 0;
                 }
                 if (pass) {
                     Cand& dst = s.cand[n_cand + pos];
-                    dst.p = cp;
-                    dst.nc6 = nc6;
-                    dst.id = g;
+                    *reinterpret_cast<float4*>(&dst.ax) = make_float4(ax, ax, c12, c12);
+                    *reinterpret_cast<float4*>(&dst.nc6) = make_float4(nc6, nc6, ay, az);
+                    s.cid[n_cand + pos] = g;
                 }
                 n_cand += npass;
             }
@@ -637,20 +933,19 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     }
     if (n_cand > 0) {
         __syncthreads();
-        warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, px, py, pz, hi, lo, nacc, wl0x, wl0y,
-                              wl0z, wh0x, wh0y, wh0z, warp_live, vmask, bul);
+        warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, L);
     }
     // 4. store
 #pragma unroll
-    for (int p = 0; p < Pol::kP; ++p) {
-        if (vmask & (1u << p)) {
-            float e;
-            if (PrecTraits<PREC>::near64)
-                e = (float)(((double)hi[p] + (double)lo[p]) + nacc[PrecTraits<PREC>::near64 ? p : 0]);
-            else
-                e = PrecTraits<PREC>::comp ? __fadd_rn(hi[p], lo[p]) : hi[p];
-            if (PREC != PREC_COUNT) e = fminf(e, kEnergyCap);
-            pol.store(w, lane, p, e);
+    for (int p = 0; p < P; ++p) {
+        if (L.vmask & (1u << p)) {
+            if (PrecTraits<PREC>::fp64) {
+                pol.store64(w, lane, p, fmin(tot_at(s, p), (double)kEnergyCap));
+            } else {
+                float e = (float)tot_at(s, p);
+                if (PREC != PREC_COUNT) e = fminf(e, kEnergyCap);
+                pol.store(w, lane, p, e);
+            }
         }
     }
     __syncthreads();

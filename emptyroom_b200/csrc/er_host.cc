@@ -17,6 +17,27 @@ static void cross(const double a[3], const double b[3], double c[3]) {
     c[2] = a[0] * b[1] - a[1] * b[0];
 }
 
+void positioning_frame(const double t[9], double r[9]) {
+    if (t[3] == 0.0 && t[6] == 0.0) {
+        for (int k = 0; k < 9; ++k) r[k] = t[k];
+        return;
+    }
+    // Gram-Schmidt on the columns a, b, c: q1 = a/|a|, q2 = b' / |b'|,
+    // q3 = q1 x q2 (a proper rotation, so handedness is kept)
+    const double a[3] = {t[0], t[3], t[6]}, b[3] = {t[1], t[4], t[7]}, c[3] = {t[2], t[5], t[8]};
+    const double la = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+    const double q1[3] = {a[0] / la, a[1] / la, a[2] / la};
+    const double r01 = q1[0] * b[0] + q1[1] * b[1] + q1[2] * b[2];
+    double bp[3] = {b[0] - r01 * q1[0], b[1] - r01 * q1[1], b[2] - r01 * q1[2]};
+    const double r11 = sqrt(bp[0] * bp[0] + bp[1] * bp[1] + bp[2] * bp[2]);
+    const double q2[3] = {bp[0] / r11, bp[1] / r11, bp[2] / r11};
+    double q3[3];
+    cross(q1, q2, q3);
+    r[0] = la;  r[1] = r01; r[2] = q1[0] * c[0] + q1[1] * c[1] + q1[2] * c[2];
+    r[3] = 0.0; r[4] = r11; r[5] = q2[0] * c[0] + q2[1] * c[1] + q2[2] * c[2];
+    r[6] = 0.0; r[7] = 0.0; r[8] = q3[0] * c[0] + q3[1] * c[1] + q3[2] * c[2];
+}
+
 void perpendicular_widths(const double t[9], double w[3]) {
     // columns of t are the cell vectors a, b, c
     const double a[3] = {t[0], t[3], t[6]}, b[3] = {t[1], t[4], t[7]}, c[3] = {t[2], t[5], t[8]};
@@ -66,6 +87,7 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
     f.n_atoms = d.n_atoms;
     for (int k = 0; k < 3; ++k) f.rep[k] = d.rep[k];
     for (int k = 0; k < 9; ++k) f.t[k] = d.t_matrix[k];
+    positioning_frame(d.t_matrix, f.r);
     f.rc2 = d.r_cutoff_squared;
     f.imgs_per_atom = (int)ipa;
     f.h = h;
@@ -95,7 +117,7 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
     std::vector<HostImage> xyz;
     std::vector<float> par;
     std::vector<uint32_t> ids;
-    const double* t = d.t_matrix;
+    const double* t = f.r;  // image positions in the positioning frame
     for (int a = 0; a < d.n_atoms; ++a) {
         const er_particle& p = d.atoms[a];
         // An atom with eps == 0 or sig == 0 adds exactly 0.0 to every sum of

@@ -19,6 +19,7 @@ struct HostFramework {
     int rep[3] = {0, 0, 0};
     int imgs_per_atom = 1;
     double t[9] = {0};
+    double r[9] = {0};                  // positioning frame (upper triangular)
     double rc2 = 0.0;
     double h = 2.0;
     int nc[3] = {1, 1, 1};
@@ -34,6 +35,10 @@ struct HostFramework {
 // Validates desc and builds the image cell list with cell edge h (A).
 int build_framework(const er_framework_desc& desc, double h, HostFramework& out,
                     std::string& err);
+
+// Upper-triangular frame r = Q^T t of the cell matrix t (Q a proper rotation):
+// r == t bit for bit when t[3] == t[6] == 0.
+void positioning_frame(const double t[9], double r[9]);
 
 // Perpendicular widths of the cell spanned by the columns of t (A).
 void perpendicular_widths(const double t[9], double w[3]);

@@ -11,7 +11,8 @@ namespace er {
 // Atom images a + T n (n in [-rep, rep]^3, the image loop of
 // src/computegridsheet.h:54-56) that can lie within the cutoff of the unit
 // cell are kept, sorted into a Cartesian cell list whose x index runs fastest,
-// so one (y, z) row of cells is one contiguous range of images.
+// so one (y, z) row of cells is one contiguous range of images. Cartesian
+// positions are taken in the frame r (the first lattice axis along x).
 struct FwDev {
     const double4* img_xyz;   // Cartesian position (x, y, z, 0), FP64, cell-sorted
     const float2* img_par;    // (C12, -C6) = (4 eps sig^12, -4 eps sig^6), FP32
@@ -24,7 +25,9 @@ struct FwDev {
     int nc[3];                // cells per axis
     double cell_lo[3];        // Cartesian corner of cell (0,0,0)
     double h, inv_h;          // cell edge (A)
-    double t[9];              // fractional -> Cartesian, row-major
+    double t[9];              // fractional -> Cartesian (the caller's cell matrix), row-major
+    double r[9];              // positioning frame: upper-triangular rotation of t (== t
+                              // when t is upper triangular); positions use r
     double rc2;               // squared cutoff, FP64 (the reference's r_cutoff_squared)
     int rep[3];
     int imgs_per_atom;        // (2 rep0 + 1)(2 rep1 + 1)(2 rep2 + 1)
@@ -48,6 +51,7 @@ struct GridTask {
     int nb[3];          // bricks per axis
     int tile_p;         // points per thread of the kernel variant (brick 2P x 8 x 16)
     float* out;         // nx*ny*nz, index k + j*nz + i*ny*nz
+    double* out64;      // same layout, FP64 (PREC_FP64 jobs only)
 };
 
 // Widom points of one framework. `order` lists the unblocked insertion indices

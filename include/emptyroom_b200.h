@@ -87,7 +87,8 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);
 #define ER_PREC_NEAR64 0x08  /* as ER_PREC_COMP, with the pairs of atoms within 5 A of
                                 a warp's points in FP64 (the default of er_henry) */
 #define ER_PREC_FP32 0x10    /* FP32 pair terms, plain FP32 accumulation */
-#define ER_PREC_FP64 0x20    /* FP64 pair terms and accumulation (precision sweeps) */
+#define ER_PREC_FP64 0x20    /* FP64 pair terms and accumulation, same pair set as the
+                                FP32 modes (precision sweeps); needs ER_OUT_F64 */
 #define ER_COUNT_PAIRS 0x40  /* diagnostic: write the number of in-cutoff pair terms per
                                 point instead of the energy (same traversal) */
 #define ER_TILE_P8 0x80      /* kernel variant with 8 points per thread (16 x 8 x 16

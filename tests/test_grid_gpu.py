@@ -273,3 +273,73 @@ def test_near64_is_more_accurate(ctx):
     # NEAR64 errors are left by the FP32 far pairs and the FP32 output rounding
     assert err64 < err32
     assert np.all(np.abs(e64 - ref)[neg] <= 2e-6 * np.abs(ref[neg]) + 2e-4)
+
+
+def _rotated(t, seed):
+    """t rotated by a seeded proper rotation (a cell matrix that is not upper
+    triangular; same lattice up to rotation, so the same energies)."""
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q = q * np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q @ np.asarray(t, dtype=np.float64).reshape(3, 3)
+
+
+@pytest.mark.parametrize("flags", [0, er.ER_TILE_P8])
+def test_rotated_cell_matches_oracle(ctx, flags):
+    f = synth.make_framework(160, (16.0, 19.0, 17.5), (75, 105, 98), 140, probe="Kr")
+    P = f.particles()
+    t = _rotated(f.t_matrix, 3)
+    assert abs(t[1, 0]) > 1e-3 and abs(t[2, 0]) > 1e-3
+    fw = ctx.upload(P, t, f.rep, f.rc2)
+    dims = (21, 18, 26)
+    e = ctx.grid(fw, dims, precision=flags)
+    ref = oracle.grid(P, t, f.rep, f.rc2, dims)
+    S = oracle.grid_abs(P, t, f.rep, f.rc2, dims)
+    _check(grid_errors(e, ref, S))
+    # the summed pair set is the reference's, exactly
+    cnt = ctx.count_pairs(fw, dims)
+    want = oracle.points_pairs(P, t, f.rep, f.rc2, oracle.lattice_points(dims))
+    assert np.array_equal(cnt.astype(np.float64).ravel(), want)
+
+
+@pytest.mark.parametrize("flags", [0, er.ER_TILE_P8])
+def test_pair_counts_exact(ctx, flags):
+    f = synth.config1(3)
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    dims = (23, 31, 17)
+    cnt = ctx.count_pairs(fw, dims) if flags == 0 else None
+    if cnt is None:
+        cnt = np.empty(dims, dtype=np.float32)
+        import ctypes
+        from emptyroom_b200 import _capi
+        assert _capi.lib().er_grid(ctx._h, fw.id, *dims, er.ER_COUNT_PAIRS | flags,
+                                   cnt.ctypes.data_as(ctypes.c_void_p)) == 0
+    want = oracle.points_pairs(P, f.t_matrix, f.rep, f.rc2, oracle.lattice_points(dims))
+    assert np.array_equal(cnt.astype(np.float64).ravel(), want)
+
+
+@pytest.mark.parametrize("flags", [0, er.ER_TILE_P8])
+def test_fp64_mode_matches_oracle(ctx, flags):
+    f = synth.make_framework(170, (18.0, 17.0, 21.0), (88, 100, 93), 160, probe="CH4")
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    dims = (19, 22, 15)
+    e = ctx.grid(fw, dims, precision=er.ER_PREC_FP64 | flags, f64=True)
+    ref = oracle.grid(P, f.t_matrix, f.rep, f.rc2, dims)
+    S = oracle.grid_abs(P, f.t_matrix, f.rep, f.rc2, dims)
+    cap = ref >= er.ER_ENERGY_CAP
+    assert np.array_equal(e >= er.ER_ENERGY_CAP, cap)
+    ok = ~cap
+    # FP64 terms summed in another order (and positions relative to a box
+    # centre): errors of a few ulps of the absolute sum
+    assert np.all(np.abs(e[ok] - ref[ok]) <= 1e-12 * S[ok] + 1e-9)
+
+
+def test_fp64_mode_needs_f64_output(ctx):
+    f = synth.config1(0)
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    with pytest.raises(er.ErError):
+        ctx.grid(fw, (4, 4, 4), precision=er.ER_PREC_FP64)
