@@ -91,7 +91,7 @@ constexpr int grid_min_blocks() {
 template <int PREC, int P>
 __global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
     grid_kernel(const __grid_constant__ GridTask task) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
     GridPolicy<P> pol(&task, blockIdx.x);
     process_cta<GridPolicy<P>, PREC>(s, pol, task.fw, task.cc);
@@ -103,7 +103,7 @@ template <int PREC>
 __global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
     grid_persistent_kernel(const GridTask* __restrict__ tasks, const WorkItem* __restrict__ items,
                            int n_items, int* head) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
     for (;;) {
         if (threadIdx.x == 0) s.item = atomicAdd(head, 1);

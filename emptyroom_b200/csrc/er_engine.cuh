@@ -64,6 +64,8 @@ struct PrecTraits {
 };
 
 constexpr int kNearCap = 128;     // near-list capacity per warp (overflow stays FP32)
+constexpr int kRec = 3;           // borderline shell atoms recorded per thread and flush
+                                  // (10-bit list positions packed in one register)
 constexpr float kNearR = 5.0f;    // near radius (A) from the warp box
 
 // One candidate atom image in shared memory (32 bytes, so a list entry can be
@@ -74,7 +76,7 @@ struct __align__(32) Cand {
     float nc6, nc6_, ay, az;     // -C6, y, z
 };
 
-struct __align__(16) EngineSmem {
+struct __align__(32) EngineSmem {
     Cand cand[kMaxCand];                   // CTA candidates
     int cid[kMaxCand];                     // their image indices (FP64 paths)
     unsigned short wl[kWarps][kMaxCand];   // per-warp inner (front) / shell (back) lists of
@@ -429,29 +431,31 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
 // Lattice shell list: cutoff tested per pair (mask 1.0 / 0.0), and the
 // smallest |r^2 - fl32(rc^2)| per point pair kept for the borderline test.
 template <class Pol, int PREC>
-__device__ __forceinline__ void lattice_shell(EngineSmem& s, const unsigned short* wl,
-                                              int n_sh, float rc2f, Lane<Pol, PREC>& L,
-                                              float* mnd) {
+__device__ __forceinline__ int lattice_shell(EngineSmem& s, const unsigned short* wl, int n_sh,
+                                             float rc2f, float win, Lane<Pol, PREC>& L,
+                                             unsigned& rec) {
     constexpr int M = Pol::kP / 2;
     constexpr bool kComp = PrecTraits<PREC>::comp;
     f2_t px2[M], acc2[M];
+    int nrec = 0;
+    rec = 0;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         px2[m] = f2_pack(L.px[2 * m], L.px[2 * m + 1]);
         acc2[m] = 0ull;
-        mnd[m] = INFINITY;
     }
     const f2_t rc2 = f2_pack(rc2f, rc2f);
     const float py = L.py[0], pz = L.pz[0];
     const char* cbase = reinterpret_cast<const char*>(s.cand);
     // the shell list runs backwards from the end of wl
     const unsigned* wl32 = reinterpret_cast<const unsigned*>(wl);
-    auto atom = [&](unsigned off) {
+    auto atom = [&](unsigned off, int q) {
         const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
         const float4 v1 = *reinterpret_cast<const float4*>(cbase + off + 16);
         const f2_t nc6 = f2_pack(v1.x, v1.y);
         const float ss = ss_lattice(py, pz, v1.z, v1.w);
         const f2_t ss2 = f2_pack(ss, ss);
+        float mn = INFINITY;
 #pragma unroll
         for (int m = 0; m < M; ++m) {
             const f2_t dx = f2_sub(px2[m], v0.x);
@@ -460,7 +464,7 @@ __device__ __forceinline__ void lattice_shell(EngineSmem& s, const unsigned shor
             f2_unpack(r2, r0, r1);
             const f2_t in = f2_pack(set_lt(r0, rc2f), set_lt(r1, rc2f));
             f2_unpack(f2_sub(r2, rc2), d0, d1);
-            mnd[m] = fminf(mnd[m], fminf(fabsf(d0), fabsf(d1)));
+            mn = fminf(mn, fminf(fabsf(d0), fabsf(d1)));
             if (PREC == PREC_COUNT) {
                 acc2[m] = f2_add(acc2[m], in);
             } else {
@@ -469,6 +473,10 @@ __device__ __forceinline__ void lattice_shell(EngineSmem& s, const unsigned shor
                 acc2[m] = f2_fma(f2_mul(u3, in), f2_fma(v0.y, u3, nc6), acc2[m]);
             }
         }
+        if (mn <= win) {  // rare: a pair of this atom sits near the cutoff
+            rec = (rec << 10) | (unsigned)q;
+            ++nrec;
+        }
     };
     int q = 0;
     while (q < n_sh) {
@@ -476,23 +484,24 @@ __device__ __forceinline__ void lattice_shell(EngineSmem& s, const unsigned shor
         for (; q + 1 < qe; q += 2) {
             // entries q, q+1 sit at wl[K-1-q], wl[K-2-q]: one aligned u32
             const unsigned two = wl32[(kMaxCand - 2 - q) >> 1];
-            atom(two >> 16);
-            atom(two & 0xffffu);
+            atom(two >> 16, q);
+            atom(two & 0xffffu, q + 1);
         }
         if (q < qe) {
-            atom(wl[kMaxCand - 1 - q]);
+            atom(wl[kMaxCand - 1 - q], q);
             ++q;
         }
         if (kComp) fold_packed<M>(s, acc2);
     }
     if (!kComp) fold_packed<M>(s, acc2);
+    return nrec;
 }
 
 // Generic (per-point x, y, z) inner and shell lists, scalar FP32.
 template <class Pol, int PREC>
-__device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned short* wl,
-                                              int n_in, int n_sh, float rc2f, float win,
-                                              Lane<Pol, PREC>& L, unsigned& bflag) {
+__device__ __forceinline__ int generic_lists(EngineSmem& s, const unsigned short* wl,
+                                             int n_in, int n_sh, float rc2f, float win,
+                                             Lane<Pol, PREC>& L, unsigned& rec) {
     constexpr int P = Pol::kP;
     constexpr bool kComp = PrecTraits<PREC>::comp;
     float acc[P];
@@ -527,9 +536,8 @@ __device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned shor
             }
         }
     }
-    bool bf[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) bf[p] = false;
+    int nrec = 0;
+    rec = 0;
     q = 0;
     while (q < n_sh) {
         const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
@@ -539,6 +547,7 @@ __device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned shor
                 reinterpret_cast<const char*>(s.cand) + wl[kMaxCand - 1 - q]);
             const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);
             const float4 v1 = *reinterpret_cast<const float4*>(&cd.nc6);
+            float mn = INFINITY;
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v1.z, v1.w);
@@ -550,7 +559,11 @@ __device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned shor
                     const float u3 = __fmul_rn(__fmul_rn(u, u), u);
                     if (dd < 0.f) acc[p] = __fmaf_rn(u3, __fmaf_rn(v0.z, u3, v1.x), acc[p]);
                 }
-                bf[p] = bf[p] || (fabsf(dd) <= win);
+                mn = fminf(mn, fabsf(dd));
+            }
+            if (mn <= win) {  // rare: a pair of this atom sits near the cutoff
+                rec = (rec << 10) | (unsigned)q;
+                ++nrec;
             }
         }
         if (kComp) {
@@ -565,30 +578,34 @@ __device__ __forceinline__ void generic_lists(EngineSmem& s, const unsigned shor
 #pragma unroll
         for (int p = 0; p < P; ++p) tot_at(s, p) += (double)acc[p];
     }
-    bflag = 0;
-#pragma unroll
-    for (int p = 0; p < P; ++p) bflag |= bf[p] ? (1u << p) : 0u;
+    return nrec;
 }
 
-// Exact re-decision of the borderline shell pairs of the points flagged in
-// bflag: a pair whose FP32 r^2 is within `win` of fl32(rc^2) is decided by
-// exact_in_cutoff, and its term added or removed where the FP32 decision
-// differed. Kept out of line: it runs for a few lanes of a few warps.
+// Exact re-decision of the borderline shell pairs: a pair whose FP32 r^2 is
+// within `win` of fl32(rc^2) is decided by exact_in_cutoff, and its term
+// added or removed where the FP32 decision differed. The shell loops record
+// the list positions of the atoms with such a pair (the last kRec of them,
+// 10 bits each, in `rec`); past kRec records the whole shell list is
+// re-examined. Kept out of line: it runs for a few
+// lanes of some warps.
 template <class Pol, int PREC>
 static __device__ __noinline__ void recheck_borderline(EngineSmem& s, const Pol& pol,
                                                        const FwDev& fw, const CutoffConsts& cc,
                                                        const unsigned short* wl, int n_sh,
-                                                       float win, unsigned bflag,
+                                                       float win, int nrec, unsigned rec,
                                                        const Lane<Pol, PREC>& L) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float rc2f = cc.rc2f;
-    for (int qq = 0; qq < n_sh; ++qq) {
-        const unsigned off = wl[kMaxCand - 1 - qq];
+    const bool all = nrec > kRec;
+    const int nq = all ? n_sh : nrec;
+    for (int r = 0; r < nq; ++r) {
+        const int q = all ? r : (int)((rec >> (10 * r)) & 1023u);
+        const unsigned off = wl[kMaxCand - 1 - q];
         const Cand& cd = s.cand[off >> 5];
         const float ss = Pol::kLattice ? ss_lattice(L.py[0], L.pz[0], cd.ay, cd.az) : 0.f;
 #pragma unroll 1
         for (int p = 0; p < Pol::kP; ++p) {
-            if (!(bflag & (1u << p))) continue;
+            if (!(L.vmask & (1u << p))) continue;
             const float r2 =
                 Pol::kLattice ? r2_lattice(L.px[p], cd.ax, ss)
                               : r2_generic(L.px[p], L.py[Pol::kLattice ? 0 : p],
@@ -681,7 +698,8 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         qz = z - o2;
     };
 
-    unsigned bflag = 0;
+    int nrec = 0;
+    unsigned rec = 0;
     if (kF64) {
         // every inner pair in FP64; shell pairs decided as below, term in FP64
         double o0, o1, o2;
@@ -716,19 +734,15 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
     }
 
     if (Pol::kLattice) {
-        float mnd[P / 2];
         lattice_inner<Pol, PREC>(s, wl, n_in, L);
-        lattice_shell<Pol, PREC>(s, wl, n_sh, rc2f, L, mnd);
-#pragma unroll
-        for (int m = 0; m < P / 2; ++m) bflag |= (mnd[m] <= win) ? (3u << (2 * m)) : 0u;
+        nrec = lattice_shell<Pol, PREC>(s, wl, n_sh, rc2f, win, L, rec);
     } else {
-        generic_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, bflag);
+        nrec = generic_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, rec);
     }
 
     // --- exact re-decision of borderline shell pairs (rare); lanes without a
     // flagged point idle through it
-    bflag &= L.vmask;
-    if (bflag) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, bflag, L);
+    if (nrec > 0) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, nrec, rec, L);
     // --- near list in FP64: exact positions (FP64 images and points relative
     // to the CTA centre) and FP64 (C12, C6); all near atoms are inner atoms.
     if (kNear && n_near > 0) {

@@ -135,7 +135,7 @@ __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_key
 
 __global__ void __launch_bounds__(kThreads, 2)
     henry_energy_kernel(const __grid_constant__ PointTask task) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     if ((long long)blockIdx.x * (kWarps * 32 * kHenryP) >= (long long)*task.n_valid) return;
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
     PointPolicy<kHenryP> pol(&task, blockIdx.x);
