@@ -248,11 +248,17 @@ int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out
     ER_CUDA(ctx, cudaEventCreate(&e1));
     float best_ms = 0.f;
     int best = 4;
+    // Both variants time the same first x-layers: a multiple of 16 large
+    // enough for four waves of the bigger (P = 8) bricks on this GPU, so
+    // neither variant is timed on an underfilled launch.
+    const int nbyz = ((ny + 2 * kWJ - 1) / (2 * kWJ)) * ((nz + 2 * kWK - 1) / (2 * kWK));
+    const int slots = 3 * ctx->num_sms;
+    const int layers = 16 * std::max(1, (4 * slots + nbyz - 1) / nbyz);
     for (int P : {4, 8}) {
         GridTask t;
         int st = fill_grid_task(ctx, f, nx, ny, nz, out, t, P);
         if (st != ER_OK) return st;
-        if (nx >= 17) t.nb[0] = 16 / (2 * P);  // the first 16 x-layers only
+        if (nx > layers) t.nb[0] = layers / (2 * P);
         float ms_min = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             ER_CUDA(ctx, cudaEventRecord(e0, ctx->stream));

@@ -70,10 +70,11 @@ constexpr float kNearR = 5.0f;    // near radius (A) from the warp box
 
 // One candidate atom image in shared memory (32 bytes, so a list entry can be
 // the byte offset of its record). x, C12 and -C6 are stored twice so that a
-// 128-bit load yields them as packed FP32x2 operands.
+// 128-bit load yields them as packed FP32x2 operands; the position is the
+// first 16 bytes (one vector load in the per-warp split).
 struct __align__(32) Cand {
-    float ax, ax_, c12, c12_;    // x, C12 (position relative to the CTA centre)
-    float nc6, nc6_, ay, az;     // -C6, y, z
+    float ax, ax_, ay, az;       // x (twice), y, z relative to the CTA centre
+    float c12, c12_, nc6, nc6_;  // C12 (twice), -C6 (twice)
 };
 
 struct __align__(32) EngineSmem {
@@ -393,15 +394,16 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
     const char* cbase = reinterpret_cast<const char*>(s.cand);
     const unsigned* wl32 = reinterpret_cast<const unsigned*>(wl);
     auto atom = [&](unsigned off) {
-        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
-        const float4 v1 = *reinterpret_cast<const float4*>(cbase + off + 16);
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);       // x x | y z
+        const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(cbase + off + 16);  // C12 | -C6
         if (PREC == PREC_COUNT) {
 #pragma unroll
             for (int m = 0; m < M; ++m) acc2[m] = f2_add(acc2[m], one2);
             return;
         }
-        const f2_t nc6 = f2_pack(v1.x, v1.y);
-        const float ss = ss_lattice(py, pz, v1.z, v1.w);
+        float ay, az;
+        f2_unpack(v0.y, ay, az);
+        const float ss = ss_lattice(py, pz, ay, az);
         const f2_t ss2 = f2_pack(ss, ss);
 #pragma unroll
         for (int m = 0; m < M; ++m) {
@@ -411,7 +413,7 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
             f2_unpack(r2, r0, r1);
             const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
             const f2_t u3 = f2_mul(f2_mul(u, u), u);
-            acc2[m] = f2_fma(u3, f2_fma(v0.y, u3, nc6), acc2[m]);
+            acc2[m] = f2_fma(u3, f2_fma(v1.x, u3, v1.y), acc2[m]);
         }
     };
     int q = 0;
@@ -450,10 +452,11 @@ __device__ __forceinline__ int lattice_shell(EngineSmem& s, const unsigned short
     // the shell list runs backwards from the end of wl
     const unsigned* wl32 = reinterpret_cast<const unsigned*>(wl);
     auto atom = [&](unsigned off, int q) {
-        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
-        const float4 v1 = *reinterpret_cast<const float4*>(cbase + off + 16);
-        const f2_t nc6 = f2_pack(v1.x, v1.y);
-        const float ss = ss_lattice(py, pz, v1.z, v1.w);
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);       // x x | y z
+        const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(cbase + off + 16);  // C12 | -C6
+        float ay, az;
+        f2_unpack(v0.y, ay, az);
+        const float ss = ss_lattice(py, pz, ay, az);
         const f2_t ss2 = f2_pack(ss, ss);
         float mn = INFINITY;
 #pragma unroll
@@ -470,7 +473,7 @@ __device__ __forceinline__ int lattice_shell(EngineSmem& s, const unsigned short
             } else {
                 const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
                 const f2_t u3 = f2_mul(f2_mul(u, u), u);
-                acc2[m] = f2_fma(f2_mul(u3, in), f2_fma(v0.y, u3, nc6), acc2[m]);
+                acc2[m] = f2_fma(f2_mul(u3, in), f2_fma(v1.x, u3, v1.y), acc2[m]);
             }
         }
         if (mn <= win) {  // rare: a pair of this atom sits near the cutoff
@@ -514,17 +517,17 @@ __device__ __forceinline__ int generic_lists(EngineSmem& s, const unsigned short
         for (; q < qe; ++q) {
             const Cand& cd = *reinterpret_cast<const Cand*>(
                 reinterpret_cast<const char*>(s.cand) + wl[q]);
-            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);
-            const float4 v1 = *reinterpret_cast<const float4*>(&cd.nc6);
+            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);   // x - y z
+            const float4 v1 = *reinterpret_cast<const float4*>(&cd.c12);  // C12 - -C6 -
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 if (PREC == PREC_COUNT) {
                     acc[p] += 1.0f;
                 } else {
-                    const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v1.z, v1.w);
+                    const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v0.z, v0.w);
                     const float u = rcp_approx(r2);
                     const float u3 = __fmul_rn(__fmul_rn(u, u), u);
-                    acc[p] = __fmaf_rn(u3, __fmaf_rn(v0.z, u3, v1.x), acc[p]);
+                    acc[p] = __fmaf_rn(u3, __fmaf_rn(v1.x, u3, v1.z), acc[p]);
                 }
             }
         }
@@ -545,19 +548,19 @@ __device__ __forceinline__ int generic_lists(EngineSmem& s, const unsigned short
         for (; q < qe; ++q) {
             const Cand& cd = *reinterpret_cast<const Cand*>(
                 reinterpret_cast<const char*>(s.cand) + wl[kMaxCand - 1 - q]);
-            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);
-            const float4 v1 = *reinterpret_cast<const float4*>(&cd.nc6);
+            const float4 v0 = *reinterpret_cast<const float4*>(&cd.ax);   // x - y z
+            const float4 v1 = *reinterpret_cast<const float4*>(&cd.c12);  // C12 - -C6 -
             float mn = INFINITY;
 #pragma unroll
             for (int p = 0; p < P; ++p) {
-                const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v1.z, v1.w);
+                const float r2 = r2_generic(L.px[p], L.py[p], L.pz[p], v0.x, v0.z, v0.w);
                 const float dd = __fsub_rn(r2, rc2f);
                 if (PREC == PREC_COUNT) {
                     if (dd < 0.f) acc[p] += 1.0f;
                 } else {
                     const float u = rcp_approx(r2);
                     const float u3 = __fmul_rn(__fmul_rn(u, u), u);
-                    if (dd < 0.f) acc[p] = __fmaf_rn(u3, __fmaf_rn(v0.z, u3, v1.x), acc[p]);
+                    if (dd < 0.f) acc[p] = __fmaf_rn(u3, __fmaf_rn(v1.x, u3, v1.z), acc[p]);
                 }
                 mn = fminf(mn, fabsf(dd));
             }
@@ -645,7 +648,8 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         const int c = base + lane;
         bool in = false, sh = false, nr = false;
         if (c < n_cand) {
-            const float ax = s.cand[c].ax, ay = s.cand[c].ay, az = s.cand[c].az;
+            const float4 a = *reinterpret_cast<const float4*>(&s.cand[c].ax);
+            const float ax = a.x, ay = a.z, az = a.w;
             const float ex = fmaxf(0.f, fmaxf(wl0x - ax, ax - wh0x));
             const float ey = fmaxf(0.f, fmaxf(wl0y - ay, ay - wh0y));
             const float ez = fmaxf(0.f, fmaxf(wl0z - az, az - wh0z));
@@ -936,8 +940,8 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                 }
                 if (pass) {
                     Cand& dst = s.cand[n_cand + pos];
-                    *reinterpret_cast<float4*>(&dst.ax) = make_float4(ax, ax, c12, c12);
-                    *reinterpret_cast<float4*>(&dst.nc6) = make_float4(nc6, nc6, ay, az);
+                    *reinterpret_cast<float4*>(&dst.ax) = make_float4(ax, ax, ay, az);
+                    *reinterpret_cast<float4*>(&dst.c12) = make_float4(c12, c12, nc6, nc6);
                     s.cid[n_cand + pos] = g;
                 }
                 n_cand += npass;
