@@ -183,7 +183,8 @@ class Context:
         self._check(_capi.lib().er_ctx_stream(self._h, ctypes.byref(v)))
         return v.value or 0
 
-    def upload(self, parts, t_matrix, rep, rc2):
+    @staticmethod
+    def _desc(parts, t_matrix, rep, rc2):
         p = np.ascontiguousarray(parts, dtype=np.float64).reshape(-1, 5)
         d = ErFrameworkDesc()
         d.n_atoms = len(p)
@@ -191,9 +192,27 @@ class Context:
         d.t_matrix[:] = [float(x) for x in np.asarray(t_matrix, dtype=np.float64).reshape(9)]
         d.rep[:] = [int(x) for x in rep]
         d.r_cutoff_squared = float(rc2)
+        return d, p
+
+    def upload(self, parts, t_matrix, rep, rc2):
+        d, p = self._desc(parts, t_matrix, rep, rc2)
         fid = ctypes.c_int(0)
         self._check(_capi.lib().er_framework_upload(self._h, ctypes.byref(d), ctypes.byref(fid)))
         return Framework(self, fid.value, len(p))
+
+    def upload_many(self, items):
+        """items: list of (particles, t_matrix, rep, rc2); one er_framework_upload_many call
+        (cell lists built on all host threads)."""
+        descs, keep = [], []
+        for it in items:
+            d, p = self._desc(*it)
+            descs.append(d)
+            keep.append(p)
+        n = len(descs)
+        arr = (ErFrameworkDesc * max(n, 1))(*descs)
+        ids = (ctypes.c_int * max(n, 1))()
+        self._check(_capi.lib().er_framework_upload_many(self._h, arr, n, ids))
+        return [Framework(self, ids[i], len(keep[i])) for i in range(n)]
 
     def grid(self, fw, dims, precision=ER_PREC_COMP, f64=False):
         """Host grid (nx, ny, nz) as float32 (or float64)."""

@@ -71,6 +71,7 @@ SIGNATURES = {
     "er_ctx_synchronize": (c_int, [c_void_p]),
     "er_ctx_stream": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
     "er_framework_upload": (c_int, [c_void_p, ctypes.POINTER(ErFrameworkDesc), _ip]),
+    "er_framework_upload_many": (c_int, [c_void_p, ctypes.POINTER(ErFrameworkDesc), c_int, _ip]),
     "er_framework_release": (c_int, [c_void_p, c_int]),
     "er_framework_bytes": (c_int, [c_void_p, c_int, ctypes.POINTER(c_size_t)]),
     "er_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),

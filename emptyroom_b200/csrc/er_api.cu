@@ -3,7 +3,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdio>
+#include <memory>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "er_ctx.h"
@@ -62,6 +67,23 @@ int cuda_error(er_ctx* ctx, cudaError_t e, const char* what) {
     return set_error(ctx, e == cudaErrorMemoryAllocation ? ER_ERR_NOMEM : ER_ERR_CUDA, m);
 }
 
+int pool_alloc(er_ctx* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), ctx->pool, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(ctx->stream);
+        cudaMemPoolTrimTo(ctx->pool, 0);
+        e = cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), ctx->pool, ctx->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            return ER_ERR_NOMEM;
+        }
+    }
+    return ER_OK;
+}
+
 const FwRecord* find_fw(er_ctx* ctx, int fw_id) {
     auto it = ctx->fws.find(fw_id);
     return it == ctx->fws.end() ? nullptr : &it->second;
@@ -99,19 +121,37 @@ __global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
 
 // One CTA per SM slot pulls (task, brick) items from the queue until it is
 // empty; each task carries its own kernel variant (4 or 8 points per thread).
+// With task_left given, the CTA that finishes a task's last brick raises the
+// task's flag in host-mapped memory (done_host), so the host can copy that
+// grid out while the kernel runs on.
+// Queue item q is brick q - start[k] of task k, start[k] <= q < start[k + 1];
+// tasks are stored longest first.
 template <int PREC>
 __global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
-    grid_persistent_kernel(const GridTask* __restrict__ tasks, const WorkItem* __restrict__ items,
-                           int n_items, int* head) {
+    grid_persistent_kernel(const GridTask* __restrict__ tasks, const int* __restrict__ start,
+                           int n_tasks, int n_items, int* head, int* task_left,
+                           volatile int* done_host) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
     for (;;) {
-        if (threadIdx.x == 0) s.item = atomicAdd(head, 1);
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(head, 1);
+            int k = 0;
+            if (it < n_items) {
+                int hi = n_tasks - 1;
+                while (k < hi) {
+                    const int mid = (k + hi + 1) >> 1;
+                    if (start[mid] <= it) k = mid; else hi = mid - 1;
+                }
+            }
+            s.item = it;
+            s.task = k;
+        }
         __syncthreads();
         const int it = s.item;
+        const WorkItem wi{s.task, it < n_items ? it - start[s.task] : 0};
         __syncthreads();
         if (it >= n_items) break;
-        const WorkItem wi = items[it];
         const GridTask* t = tasks + wi.task;
         if (t->tile_p == 8) {
             GridPolicy<8> pol(t, wi.brick);
@@ -119,6 +159,14 @@ __global__ void __launch_bounds__(kThreads, grid_min_blocks<PREC>())
         } else {
             GridPolicy<4> pol(t, wi.brick);
             process_cta<GridPolicy<4>, PREC>(s, pol, t->fw, t->cc);
+        }
+        if (task_left) {
+            __threadfence();  // this thread's grid stores, device-wide
+            __syncthreads();
+            if (threadIdx.x == 0 && atomicSub(&task_left[wi.task], 1) == 1) {
+                __threadfence_system();
+                done_host[wi.task] = 1;
+            }
         }
     }
 }
@@ -205,8 +253,9 @@ int launch_grid_plain(er_ctx* ctx, const GridTask& t, int prec) {
     return launch_grid_plain_on(ctx, t, prec, ctx->stream);
 }
 
-int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const WorkItem* d_items,
-                           int n_items, int* d_head, int prec) {
+int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const int* d_start, int n_tasks,
+                           int n_items, int* d_head, int prec, int* task_left = nullptr,
+                           int* done_dev = nullptr) {
     const size_t smem = sizeof(EngineSmem);
     int per_sm = 0;
     ER_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -216,11 +265,11 @@ int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const WorkItem*
     ER_CUDA(ctx, cudaMemsetAsync(d_head, 0, sizeof(int), ctx->stream));
     cudaStream_t st = ctx->stream;
     if (prec == PREC_FP32)
-        grid_persistent_kernel<PREC_FP32><<<grid, kThreads, smem, st>>>(d_tasks, d_items, n_items,
-                                                                        d_head);
+        grid_persistent_kernel<PREC_FP32><<<grid, kThreads, smem, st>>>(
+            d_tasks, d_start, n_tasks, n_items, d_head, task_left, done_dev);
     else
-        grid_persistent_kernel<PREC_COMP><<<grid, kThreads, smem, st>>>(d_tasks, d_items, n_items,
-                                                                        d_head);
+        grid_persistent_kernel<PREC_COMP><<<grid, kThreads, smem, st>>>(
+            d_tasks, d_start, n_tasks, n_items, d_head, task_left, done_dev);
     ER_CUDA(ctx, cudaGetLastError());
     return ER_OK;
 }
@@ -309,8 +358,33 @@ int er_ctx_create(int device, er_ctx** out) {
         delete ctx;
         return ER_ERR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return ER_ERR_CUDA;
+    }
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool
+        if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+            cudaStreamDestroy(ctx->copy_stream);
+            cudaStreamDestroy(ctx->stream);
+            delete ctx;
+            return ER_ERR_CUDA;
+        }
+    }
     int st = configure_kernels(ctx);
     if (st != ER_OK) {
+        cudaMemPoolDestroy(ctx->pool);
+        cudaStreamDestroy(ctx->copy_stream);
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return st;
@@ -323,14 +397,22 @@ void er_ctx_destroy(er_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (auto& kv : ctx->fws) cudaFree(kv.second.block);
+    cudaStreamSynchronize(ctx->copy_stream);
+    for (auto& kv : ctx->fws) cudaFreeAsync(kv.second.block, ctx->stream);
     ctx->fws.clear();
-    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->tasks,  &ctx->items,  &ctx->counter,
+    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->counter,
                       &ctx->p_grid,   &ctx->p_lab,  &ctx->p_seg,  &ctx->p_flags,
                       &ctx->p_misc,   &ctx->p_mask, &ctx->sheet_cache.grid};
     for (DevBuf* b : bufs) b->release();
     ctx->henry.release();
     ctx->pinned.release();
+    ctx->plan_pinned.release();
+    ctx->task_left.release();
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolDestroy(ctx->pool);
+    if (ctx->done_host) cudaFreeHost(ctx->done_host);
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -349,56 +431,57 @@ int er_ctx_stream(er_ctx* ctx, void** stream) {
     return ER_OK;
 }
 
-int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) {
-    if (!ctx || !desc || !fw_id) return ER_ERR_INVALID;
-    ER_CUDA(ctx, cudaSetDevice(ctx->device));
-    HostFramework hf;
-    std::string err;
-    int st = build_framework(*desc, ctx->cell_edge, hf, err);
-    if (st != ER_OK) return set_error(ctx, st, err);
+}  // extern "C"
+
+namespace er {
+
+// Byte layout of one framework's device block (every array 256-byte aligned).
+struct FwLayout {
+    size_t o_par, o_id, o_cs, o_af, o_lj, total;
+};
+
+static FwLayout fw_layout(const HostFramework& hf) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t n_img = hf.img_xyz.size();
+    FwLayout L;
     const size_t s_xyz = al(std::max<size_t>(n_img, 1) * sizeof(HostImage));
     const size_t s_par = al(std::max<size_t>(n_img, 1) * 2 * sizeof(float));
     const size_t s_id = al(std::max<size_t>(n_img, 1) * sizeof(uint32_t));
     const size_t s_cs = al(hf.cell_start.size() * sizeof(int));
     const size_t s_af = al(std::max<size_t>(hf.atom_frac.size(), 1) * sizeof(HostImage));
     const size_t s_lj = al(std::max<size_t>(hf.atom_lj64.size(), 2) * sizeof(double));
-    const size_t total = s_xyz + s_par + s_id + s_cs + s_af + s_lj;
-    FwRecord rec;
-    if (cudaMalloc(&rec.block, total) != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(ctx, ER_ERR_NOMEM, "framework upload: device allocation failed");
-    }
-    // one pinned host image of the whole block, one copy
-    if (ctx->pinned.ensure(total) != ER_OK) {
-        cudaFree(rec.block);
-        return set_error(ctx, ER_ERR_NOMEM, "framework upload: pinned staging failed");
-    }
-    const size_t o_par = s_xyz, o_id = o_par + s_par, o_cs = o_id + s_id, o_af = o_cs + s_cs,
-                 o_lj = o_af + s_af;
-    char* h = (char*)ctx->pinned.ptr;
+    L.o_par = s_xyz;
+    L.o_id = L.o_par + s_par;
+    L.o_cs = L.o_id + s_id;
+    L.o_af = L.o_cs + s_cs;
+    L.o_lj = L.o_af + s_af;
+    L.total = L.o_lj + s_lj;
+    return L;
+}
+
+// Writes the host image of the device block at h.
+static void fw_stage(const HostFramework& hf, const FwLayout& L, char* h) {
+    const size_t n_img = hf.img_xyz.size();
     memcpy(h, hf.img_xyz.data(), n_img * sizeof(HostImage));
-    memcpy(h + o_par, hf.img_par.data(), n_img * 2 * sizeof(float));
-    memcpy(h + o_id, hf.img_id.data(), n_img * sizeof(uint32_t));
-    memcpy(h + o_cs, hf.cell_start.data(), hf.cell_start.size() * sizeof(int));
-    memcpy(h + o_af, hf.atom_frac.data(), hf.atom_frac.size() * sizeof(HostImage));
-    memcpy(h + o_lj, hf.atom_lj64.data(), hf.atom_lj64.size() * sizeof(double));
-    cudaError_t e = cudaMemcpyAsync(rec.block, h, total, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) {
-        cudaFree(rec.block);
-        return cuda_error(ctx, e, "framework upload: copy");
-    }
-    char* b = (char*)rec.block;
+    memcpy(h + L.o_par, hf.img_par.data(), n_img * 2 * sizeof(float));
+    memcpy(h + L.o_id, hf.img_id.data(), n_img * sizeof(uint32_t));
+    memcpy(h + L.o_cs, hf.cell_start.data(), hf.cell_start.size() * sizeof(int));
+    memcpy(h + L.o_af, hf.atom_frac.data(), hf.atom_frac.size() * sizeof(HostImage));
+    memcpy(h + L.o_lj, hf.atom_lj64.data(), hf.atom_lj64.size() * sizeof(double));
+}
+
+// Fills the handle record of a framework whose block is (being) copied to `block`.
+static void fw_record(const HostFramework& hf, const FwLayout& L, void* block, FwRecord& rec) {
+    rec.block = block;
+    char* b = (char*)block;
     FwDev& d = rec.dev;
     d.img_xyz = (const double4*)b;
-    d.img_par = (const float2*)(b + o_par);
-    d.img_id = (const uint32_t*)(b + o_id);
-    d.cell_start = (const int*)(b + o_cs);
-    d.atom_frac = (const double4*)(b + o_af);
-    d.atom_lj64 = (const double2*)(b + o_lj);
-    d.n_img = (int)n_img;
+    d.img_par = (const float2*)(b + L.o_par);
+    d.img_id = (const uint32_t*)(b + L.o_id);
+    d.cell_start = (const int*)(b + L.o_cs);
+    d.atom_frac = (const double4*)(b + L.o_af);
+    d.atom_lj64 = (const double2*)(b + L.o_lj);
+    d.n_img = (int)hf.img_xyz.size();
     d.n_atoms = hf.n_atoms;
     for (int k = 0; k < 3; ++k) {
         d.nc[k] = hf.nc[k];
@@ -411,7 +494,7 @@ int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) 
     for (int k = 0; k < 9; ++k) d.r[k] = hf.r[k];
     d.rc2 = hf.rc2;
     d.imgs_per_atom = hf.imgs_per_atom;
-    rec.bytes = total;
+    rec.bytes = L.total;
     rec.rc2 = hf.rc2;
     for (int k = 0; k < 9; ++k) rec.t[k] = hf.t[k];
     for (int k = 0; k < 3; ++k)
@@ -421,9 +504,87 @@ int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) 
                       hf.t[1] * (hf.t[3] * hf.t[8] - hf.t[5] * hf.t[6]) +
                       hf.t[2] * (hf.t[3] * hf.t[7] - hf.t[4] * hf.t[6]));
     rec.n_atoms = hf.n_atoms;
-    const int id = ctx->next_fw++;
-    ctx->fws[id] = rec;
-    *fw_id = id;
+}
+
+// Runs f(i) for i in [0, n) on up to hardware_concurrency host threads.
+template <class F>
+static void parallel_for(int n, F&& f) {
+    const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+        for (int i; (i = next.fetch_add(1)) < n;) f(i);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+}
+
+}  // namespace er
+
+extern "C" {
+
+int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) {
+    if (!ctx || !desc || !fw_id) return ER_ERR_INVALID;
+    return er_framework_upload_many(ctx, desc, 1, fw_id);
+}
+
+int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids) {
+    if (!ctx || n < 0 || (n > 0 && (!descs || !fw_ids))) return ER_ERR_INVALID;
+    if (n == 0) return ER_OK;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    // 1. image cell lists, built on the host threads
+    std::vector<HostFramework> hfs(n);
+    std::vector<std::string> errs(n);
+    std::vector<int> sts(n, ER_OK);
+    const double h = ctx->cell_edge;
+    parallel_for(n, [&](int i) { sts[i] = build_framework(descs[i], h, hfs[i], errs[i]); });
+    for (int i = 0; i < n; ++i)
+        if (sts[i] != ER_OK)
+            return set_error(ctx, sts[i],
+                             n > 1 ? "framework " + std::to_string(i) + ": " + errs[i] : errs[i]);
+    // 2. device blocks and one pinned host image of all of them
+    std::vector<FwLayout> lay(n);
+    std::vector<size_t> at(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        lay[i] = fw_layout(hfs[i]);
+        at[i + 1] = at[i] + lay[i].total;
+    }
+    std::vector<void*> blocks(n, nullptr);
+    auto free_blocks = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        for (void* b : blocks)
+            if (b) cudaFreeAsync(b, ctx->stream);
+    };
+    for (int i = 0; i < n; ++i)
+        if (pool_alloc(ctx, &blocks[i], lay[i].total) != ER_OK) {
+            free_blocks();
+            return set_error(ctx, ER_ERR_NOMEM, "framework upload: device allocation failed");
+        }
+    if (ctx->pinned.ensure(at[n]) != ER_OK) {
+        free_blocks();
+        return set_error(ctx, ER_ERR_NOMEM, "framework upload: pinned staging failed");
+    }
+    char* h0 = (char*)ctx->pinned.ptr;
+    parallel_for(n, [&](int i) { fw_stage(hfs[i], lay[i], h0 + at[i]); });
+    // 3. one copy per framework, one wait
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(blocks[i], h0 + at[i], lay[i].total, cudaMemcpyHostToDevice,
+                            ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(ctx->stream);
+        free_blocks();
+        return cuda_error(ctx, e, "framework upload: copy");
+    }
+    for (int i = 0; i < n; ++i) {
+        FwRecord rec;
+        fw_record(hfs[i], lay[i], blocks[i], rec);
+        const int id = ctx->next_fw++;
+        ctx->fws[id] = rec;
+        fw_ids[i] = id;
+    }
     return ER_OK;
 }
 
@@ -431,8 +592,9 @@ int er_framework_release(er_ctx* ctx, int fw_id) {
     if (!ctx) return ER_ERR_INVALID;
     auto it = ctx->fws.find(fw_id);
     if (it == ctx->fws.end()) return set_error(ctx, ER_ERR_NOT_FOUND, "unknown framework id");
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(it->second.block);
+    // no work of this process may still read the block (as with cudaFree)
+    cudaDeviceSynchronize();
+    cudaFreeAsync(it->second.block, ctx->stream);
     ctx->fws.erase(it);
     if (ctx->sheet_cache.fw == fw_id) ctx->sheet_cache.fw = 0;
     return ER_OK;
@@ -551,11 +713,13 @@ struct er_batch_plan {
     er_ctx* ctx = nullptr;
     int mode = ER_BATCH_PERSISTENT;
     int n_jobs = 0;
-    std::vector<GridTask> tasks;
-    GridTask* d_tasks = nullptr;
-    WorkItem* d_items = nullptr;
-    int n_items = 0;
+    std::vector<GridTask> tasks;   // job order
+    std::vector<int> order;        // queue position -> job (longest first)
+    void* d_block = nullptr;       // one pool allocation: tasks, start, head
+    GridTask* d_tasks = nullptr;   // queue order
+    int* d_start = nullptr;        // n_jobs + 1 brick offsets, queue order
     int* d_head = nullptr;
+    int n_items = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
@@ -563,18 +727,13 @@ struct er_batch_plan {
 
 namespace er {
 
-// Longest-first order of (task, brick) items: bricks of denser frameworks and
-// bigger grids first, so the persistent queue drains with a short tail.
-static void build_items(const std::vector<GridTask>& tasks, const std::vector<double>& cost,
-                        std::vector<WorkItem>& items) {
-    std::vector<int> order(tasks.size());
+// Longest-first order of the jobs: bricks of denser frameworks (more atoms
+// per A^3, so more pairs per point) go first, so the tail of the persistent
+// queue holds the cheap bricks.
+static void queue_order(const std::vector<double>& cost, std::vector<int>& order) {
+    order.resize(cost.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    items.clear();
-    for (int ti : order) {
-        const int64_t nb = task_bricks(tasks[ti]);
-        for (int64_t b = 0; b < nb; ++b) items.push_back(WorkItem{ti, (int)b});
-    }
 }
 
 static int plan_enqueue(er_batch_plan* p) {
@@ -586,15 +745,22 @@ static int plan_enqueue(er_batch_plan* p) {
         }
         return ER_OK;
     }
-    return launch_grid_persistent(ctx, p->d_tasks, p->d_items, p->n_items, p->d_head, PREC_COMP);
+    return launch_grid_persistent(ctx, p->d_tasks, p->d_start, p->n_jobs, p->n_items, p->d_head,
+                                  PREC_COMP);
 }
 
 }  // namespace er
 
 extern "C" {
 
-int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode,
-                         er_batch_plan** out) {
+}  // extern "C"
+
+namespace er {
+
+// Builds a plan; with capture, the launch sequence is also captured as a graph
+// (er_batch_plan_run replays it).
+int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool capture,
+                er_batch_plan** out) {
     if (!ctx || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return ER_ERR_INVALID;
     const bool autotune = (mode & ER_BATCH_AUTOTUNE) != 0;
     mode &= ~ER_BATCH_AUTOTUNE;
@@ -630,28 +796,45 @@ int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int m
         // per-brick cost ~ atom density * cutoff volume
         cost.push_back((double)f->dev.n_img / std::max(1.0, f->volume));
     }
-    std::vector<WorkItem> items;
-    build_items(p->tasks, cost, items);
-    p->n_items = (int)items.size();
+    queue_order(cost, p->order);
     auto fail = [&](int st, const char* m) {
         er_batch_plan_destroy(p);
         return set_error(ctx, st, m);
     };
-    if (cudaMalloc(&p->d_tasks, std::max<size_t>(1, p->tasks.size()) * sizeof(GridTask)) !=
-            cudaSuccess ||
-        cudaMalloc(&p->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)) !=
-            cudaSuccess ||
-        cudaMalloc(&p->d_head, sizeof(int)) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ER_ERR_NOMEM, "batch: device allocation failed");
+    // queue-ordered tasks and brick offsets, staged in pinned memory, one copy
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t s_tasks = al(std::max(n_jobs, 1) * sizeof(GridTask));
+    const size_t s_start = al((size_t)(n_jobs + 1) * sizeof(int));
+    const size_t total = s_tasks + s_start + sizeof(int);
+    if (ctx->plan_pinned.ensure(total) != ER_OK)
+        return fail(ER_ERR_NOMEM, "batch: pinned staging failed");
+    char* h = (char*)ctx->plan_pinned.ptr;
+    GridTask* ht = (GridTask*)h;
+    int* hs = (int*)(h + s_tasks);
+    int64_t acc = 0;
+    for (int q = 0; q < n_jobs; ++q) {
+        ht[q] = p->tasks[p->order[q]];
+        hs[q] = (int)acc;
+        acc += task_bricks(ht[q]);
+        if (acc > INT32_MAX) return fail(ER_ERR_LIMIT, "batch: more than 2^31 bricks");
     }
-    if (!p->tasks.empty() &&
-        cudaMemcpy(p->d_tasks, p->tasks.data(), p->tasks.size() * sizeof(GridTask),
-                   cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail(ER_ERR_CUDA, "batch: task upload failed");
-    if (!items.empty() && cudaMemcpy(p->d_items, items.data(), items.size() * sizeof(WorkItem),
-                                     cudaMemcpyHostToDevice) != cudaSuccess)
+    hs[n_jobs] = (int)acc;
+    p->n_items = (int)acc;
+    if (pool_alloc(ctx, &p->d_block, total) != ER_OK)
+        return fail(ER_ERR_NOMEM, "batch: device allocation failed");
+    p->d_tasks = (GridTask*)p->d_block;
+    p->d_start = (int*)((char*)p->d_block + s_tasks);
+    p->d_head = (int*)((char*)p->d_block + s_tasks + s_start);
+    if (cudaMemcpyAsync(p->d_block, h, s_tasks + s_start, cudaMemcpyHostToDevice, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
         return fail(ER_ERR_CUDA, "batch: queue upload failed");
+    }
+    if (!capture) {
+        *out = p;
+        return ER_OK;
+    }
     // capture the launch sequence once as a CUDA graph
     cudaStream_t cs = ctx->stream;
     if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
@@ -684,7 +867,17 @@ int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int m
     return ER_OK;
 }
 
+}  // namespace er
+
+extern "C" {
+
+int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode,
+                         er_batch_plan** out) {
+    return plan_create(ctx, jobs, n_jobs, mode, true, out);
+}
+
 int er_batch_plan_run(er_batch_plan* p) {
+    if (p && !p->exec) return ER_ERR_INVALID;
     if (!p) return ER_ERR_INVALID;
     ER_CUDA(p->ctx, cudaGraphLaunch(p->exec, p->ctx->stream));
     return ER_OK;
@@ -707,16 +900,15 @@ void er_batch_plan_destroy(er_batch_plan* p) {
     if (p->ctx) cudaStreamSynchronize(p->ctx->stream);
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
-    if (p->d_tasks) cudaFree(p->d_tasks);
-    if (p->d_items) cudaFree(p->d_items);
-    if (p->d_head) cudaFree(p->d_head);
+    if (p->d_block) cudaFreeAsync(p->d_block, p->ctx->stream);
     delete p;
 }
 
 int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
     if (!ctx || n_jobs < 0 || (n_jobs > 0 && !jobs)) return ER_ERR_INVALID;
     if (mode & ER_BATCH_HOST_OUT) {
-        // stage every grid in one device buffer, run, copy each back
+        // stage every grid in one device buffer; copy each back as soon as
+        // the persistent kernel reports its last brick done
         std::vector<er_grid_job> dj(jobs, jobs + n_jobs);
         std::vector<size_t> off(n_jobs + 1, 0);
         for (int i = 0; i < n_jobs; ++i) {
@@ -729,13 +921,78 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
             return set_error(ctx, ER_ERR_NOMEM, "batch: device staging allocation failed");
         float* base = (float*)ctx->grid_f32.ptr;
         for (int i = 0; i < n_jobs; ++i) dj[i].out_device = base + off[i];
-        int st = er_grid_batch(ctx, dj.data(), n_jobs, mode & ~ER_BATCH_HOST_OUT);
+        const int inner = mode & ~ER_BATCH_HOST_OUT;
+        auto copy_out = [&](int i) {
+            return cudaMemcpyAsync(jobs[i].out_device, base + off[i],
+                                   (off[i + 1] - off[i]) * sizeof(float), cudaMemcpyDeviceToHost,
+                                   ctx->copy_stream);
+        };
+        if ((inner & ~ER_BATCH_AUTOTUNE) != ER_BATCH_PERSISTENT || n_jobs == 0) {
+            int st = er_grid_batch(ctx, dj.data(), n_jobs, inner);
+            if (st != ER_OK) return st;
+            for (int i = 0; i < n_jobs; ++i) ER_CUDA(ctx, copy_out(i));
+            ER_CUDA(ctx, cudaStreamSynchronize(ctx->copy_stream));
+            return ER_OK;
+        }
+        er_batch_plan* p = nullptr;
+        int st = plan_create(ctx, dj.data(), n_jobs, inner, false, &p);
         if (st != ER_OK) return st;
-        for (int i = 0; i < n_jobs; ++i)
-            ER_CUDA(ctx, cudaMemcpyAsync(jobs[i].out_device, base + off[i],
-                                         (off[i + 1] - off[i]) * sizeof(float),
-                                         cudaMemcpyDeviceToHost, ctx->stream));
-        ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        std::unique_ptr<er_batch_plan, void (*)(er_batch_plan*)> guard(p, er_batch_plan_destroy);
+        // bricks left per queue position, and the host-visible flags
+        std::vector<int> left(n_jobs);
+        for (int q = 0; q < n_jobs; ++q) left[q] = (int)task_bricks(p->tasks[p->order[q]]);
+        if (ctx->task_left.ensure((size_t)n_jobs * sizeof(int)) != ER_OK)
+            return set_error(ctx, ER_ERR_NOMEM, "batch: device allocation failed");
+        if (ctx->done_cap < (size_t)n_jobs) {
+            if (ctx->done_host) cudaFreeHost(ctx->done_host);
+            ctx->done_host = ctx->done_dev = nullptr;
+            ctx->done_cap = 0;
+            void* hp = nullptr;
+            if (cudaHostAlloc(&hp, (size_t)n_jobs * sizeof(int), cudaHostAllocMapped) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                return set_error(ctx, ER_ERR_NOMEM, "batch: mapped flag allocation failed");
+            }
+            void* dp = nullptr;
+            ER_CUDA(ctx, cudaHostGetDevicePointer(&dp, hp, 0));
+            ctx->done_host = (int*)hp;
+            ctx->done_dev = (int*)dp;
+            ctx->done_cap = (size_t)n_jobs;
+        }
+        volatile int* done = ctx->done_host;
+        for (int i = 0; i < n_jobs; ++i) done[i] = 0;
+        int* d_left = (int*)ctx->task_left.ptr;
+        ER_CUDA(ctx, cudaMemcpyAsync(d_left, left.data(), (size_t)n_jobs * sizeof(int),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+        st = launch_grid_persistent(ctx, p->d_tasks, p->d_start, n_jobs, p->n_items, p->d_head,
+                                    PREC_COMP, d_left, ctx->done_dev);
+        if (st != ER_OK) return st;
+        cudaEvent_t fin;
+        ER_CUDA(ctx, cudaEventCreateWithFlags(&fin, cudaEventDisableTiming));
+        cudaError_t e = cudaEventRecord(fin, ctx->stream);
+        std::vector<char> sent(n_jobs, 0);
+        int n_sent = 0;
+        // Poll until every grid is on its way; bounded by the kernel, which
+        // has no device-side waits and so always finishes.
+        while (e == cudaSuccess && n_sent < n_jobs) {
+            const cudaError_t q = cudaEventQuery(fin);
+            if (q != cudaSuccess && q != cudaErrorNotReady) {
+                e = q;
+                break;
+            }
+            const bool all = q == cudaSuccess;
+            for (int k = 0; k < n_jobs && e == cudaSuccess; ++k)
+                if (!sent[k] && (all || done[k])) {
+                    e = copy_out(p->order[k]);
+                    sent[k] = 1;
+                    ++n_sent;
+                }
+            if (!all && n_sent < n_jobs) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+        cudaEventDestroy(fin);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->copy_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "batch: run / copy-out");
         return ER_OK;
     }
     er_batch_plan* p = nullptr;

@@ -67,6 +67,7 @@ struct er_ctx {
     int device = 0;
     int num_sms = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // device->host copies overlapping the kernels
     std::string last_error;
     std::map<int, er::FwRecord> fws;
     int next_fw = 1;
@@ -74,10 +75,14 @@ struct er_ctx {
     std::map<std::tuple<int, int, int>, int> tune;  // autotuned kernel variant per job class
     // scratch
     er::DevBuf grid_f32;     // staging for host-bound grids
-    er::DevBuf tasks;        // GridTask arrays for batches
-    er::DevBuf items;        // WorkItem queues
-    er::DevBuf counter;      // persistent-queue heads
+    er::DevBuf counter;      // scratch of the FP32 rate probe
     er::HostBuf pinned;      // pinned staging
+    er::HostBuf plan_pinned; // pinned staging of batch-plan queues
+    cudaMemPool_t pool = nullptr;  // stream-ordered pool (framework blocks, plan queues)
+    er::DevBuf task_left;    // per-job bricks left (completion notification)
+    int* done_host = nullptr;   // mapped pinned per-job completion flags
+    int* done_dev = nullptr;    // the same flags, device address
+    size_t done_cap = 0;
     // Widom scratch
     er::HenryScratch henry;
     // pocket-blocking scratch
@@ -92,6 +97,9 @@ struct er_ctx {
 namespace er {
 
 int set_error(er_ctx* ctx, int status, const std::string& msg);
+// Device memory from the context's pool, ordered on ctx->stream; the pool
+// keeps freed memory for reuse (trimmed and retried once when exhausted).
+int pool_alloc(er_ctx* ctx, void** p, size_t bytes);
 int cuda_error(er_ctx* ctx, cudaError_t e, const char* what);
 const FwRecord* find_fw(er_ctx* ctx, int fw_id);
 // Cutoff constants for a framework and a CTA box diagonal (A).

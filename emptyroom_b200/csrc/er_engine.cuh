@@ -90,7 +90,7 @@ struct __align__(32) EngineSmem {
     double red[kWarps][6];
     double box[6];                         // CTA box (FP64 lo, hi)
     float wbox[kWarps][6];                 // warp boxes (local FP32 lo, hi)
-    int item;
+    int item, task;                        // persistent-queue item and its task
 };
 
 // ----------------------------------------------------------- packed FP32x2

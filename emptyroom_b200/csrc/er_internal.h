@@ -66,7 +66,7 @@ struct PointTask {
     float* energies;         // E per insertion (insertion order)
 };
 
-// Persistent batch work item: (task index, brick index).
+// Persistent-queue item as the kernel decodes it: (task position, brick).
 struct WorkItem {
     int task;
     int brick;

@@ -73,6 +73,11 @@ int er_ctx_stream(er_ctx* ctx, void** stream);
  * list. Replaces the cudaMalloc/cudaMemcpy of FrameworkParticle[] at
  * src/writegrid.cu:187-189 and src/henry.cu:133-135. *fw_id receives a handle. */
 int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id);
+/* Uploads n frameworks at once: the image cell lists are built on all host
+ * threads, staged in one pinned buffer and copied with one wait. On error no
+ * handle is created. (No counterpart in the reference, which reads one
+ * framework per process.) */
+int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids);
 int er_framework_release(er_ctx* ctx, int fw_id);
 /* Device bytes held by a framework handle. */
 int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);

@@ -343,3 +343,47 @@ def test_fp64_mode_needs_f64_output(ctx):
     fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
     with pytest.raises(er.ErError):
         ctx.grid(fw, (4, 4, 4), precision=er.ER_PREC_FP64)
+
+
+@pytest.mark.parametrize("mode", [er.ER_BATCH_PERSISTENT, er.ER_BATCH_PLAIN,
+                                  er.ER_BATCH_PERSISTENT | er.ER_BATCH_AUTOTUNE])
+def test_batch_host_out_matches_device(ctx, mode):
+    """HOST_OUT copies each grid back while the kernel still runs (persistent
+    mode); the host grids equal the device-batch grids bit for bit."""
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=14, seed=120)
+    outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)],
+                   mode & ~er.ER_BATCH_HOST_OUT)
+    hosts = [torch.full(f.dims, float("nan"), dtype=torch.float32, pin_memory=True)
+             for f in fws]
+    for rep in range(2):  # the second call reuses the flag and staging buffers
+        for h in hosts:
+            h.fill_(float("nan"))
+        ctx.grid_batch([(u, f.dims, h.data_ptr()) for u, f, h in zip(ups, fws, hosts)],
+                       mode | er.ER_BATCH_HOST_OUT)
+        for o, h in zip(outs, hosts):
+            assert torch.equal(o.cpu(), h)
+
+
+def test_upload_many_equals_single_uploads(ctx):
+    fws = synth.config2(n_frameworks=9, seed=130, spacing_range=(0.9, 1.6))
+    many = ctx.upload_many([(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws])
+    assert len({u.id for u in many}) == len(fws)
+    for f, u in zip(fws, many):
+        single = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+        assert u.device_bytes == single.device_bytes
+        assert np.array_equal(ctx.grid(u, f.dims), ctx.grid(single, f.dims))
+        single.release()
+    for u in many:
+        u.release()
+
+
+def test_upload_many_reports_the_bad_framework(ctx):
+    fws = synth.config2(n_frameworks=3, seed=131, spacing_range=(0.9, 1.6))
+    items = [(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
+    bad = items[1][0].copy()
+    bad[0, 3] = -1.0  # negative epsilon
+    items[1] = (bad,) + items[1][1:]
+    with pytest.raises(er.ErError, match="framework 1"):
+        ctx.upload_many(items)
