@@ -306,6 +306,12 @@ def run_ours(args, ws, rank, local, pg):
         "plain": {"value": plain_value, "unit": "pair-terms/s", "launches_per_step": plain_launches,
                   "batched_over_plain": value / plain_value},
     }
+    # the Widom and serving forms of the metric, at N = 1 (the batch above is
+    # the scaled workload)
+    if ws == 1 and not args.no_widom:
+        line["widom"] = run_widom(ctx, args)
+    if ws == 1 and not args.no_serving:
+        line["serving"] = run_serving(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         starts = np.cumsum([0] + [int(np.prod(f.dims)) for f in fws])
 
@@ -319,6 +325,106 @@ def run_ours(args, ws, rank, local, pg):
         line["cpu_baseline"] = cpu_baseline(fws, sheet_pairs)
     ctx.close()
     return line
+
+
+def run_widom(ctx, args):
+    """Widom batch (config 4): per framework the 0.2 A grid, its pocket mask by
+    GPU connected-components labelling, then er_henry with that device mask;
+    64 frameworks x 1e7 insertions, Xe at 298 K."""
+    import torch
+
+    from emptyroom_b200 import synth
+    T = 298.0
+    fws = synth.config4(args.widom_frameworks)
+    ups = ctx.upload_many([(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws])
+    dims = fws[0].dims
+    g = torch.empty(dims, dtype=torch.float32, device="cuda")
+    m = torch.empty(dims, dtype=torch.uint8, device="cuda")
+    cnt = torch.empty(dims, dtype=torch.float32, device="cuda")
+    n_ins = int(args.insertions)
+    s = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    def one(k, u):
+        ctx.grid_device(u, dims, g.data_ptr())
+        n_p = ctx.block_pockets_device(g.data_ptr(), dims, T, m.data_ptr())
+        r = ctx.henry_device_mask(u, T, n_ins, k, m.data_ptr(), dims)
+        return n_p, r
+
+    one(0, ups[0])  # warm-up
+    ctx.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(s)
+    res = [one(k, u) for k, u in enumerate(ups)]
+    e1.record(s)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    dev = e0.elapsed_time(e1) * 1e-3
+    # pair terms: exact for the grids; for the insertions the grid's mean
+    # in-cutoff pairs per point (insertions are uniform in the cell)
+    grid_pairs = ins_pairs = 0.0
+    for u in ups:
+        ctx.count_pairs_device(u, dims, cnt.data_ptr())
+        ctx.synchronize()
+        c = float(cnt.double().sum().item())
+        grid_pairs += c
+        ins_pairs += c / float(np.prod(dims)) * n_ins
+    for u in ups:
+        u.release()
+    total_ins = n_ins * len(fws)
+    return {"workload": f"{len(fws)} config-1 cells, Xe 298 K: 0.2 A grid {list(dims)} -> "
+                        f"GPU pocket mask -> {n_ins:.0e} Philox insertions each (config 4)",
+            "insertions_per_s": total_ins / dev, "unit": "insertions/s",
+            "ms_per_step": dev * 1e3, "wall_ms_per_step": wall * 1e3,
+            "pair_terms_per_s": (grid_pairs + ins_pairs) / dev,
+            "pair_terms_note": "grid pairs exact; insertion pairs = insertions x grid mean",
+            "n_pockets_total": int(sum(r[0] for r in res)),
+            "n_blocked_total": int(sum(r[1]["n_blocked"] for r in res)),
+            "kh_mol_m3_pa_first": res[0][1]["kh_mol_m3_pa"]}
+
+
+def run_serving(ctx, args):
+    """Serving (config 5): a Poisson stream of grid and Henry jobs replayed
+    against the request server with 8 slots and against the plain
+    one-job-at-a-time loop (1 slot); latency = finish - submit per job. Grid
+    jobs leave their grids resident in the server's device cache."""
+    from emptyroom_b200 import serve, synth
+    fws, jobs = synth.config5_stream(seconds=args.serve_seconds)
+    descs = [serve.framework_desc(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
+
+    def schedule():
+        out = []
+        for j in jobs:
+            d = descs[j["fw"]]
+            if j["kind"] == "grid":
+                out.append((j["t"], lambda srv, j=j, d=d: srv.submit_grid(j["fw"], d, j["dims"])))
+            else:
+                out.append((j["t"], lambda srv, j=j, d=d: srv.submit_henry(
+                    j["fw"], d, 298.0, j["n_ins"], j["seed"])))
+        return out
+
+    res = {"workload": f"Poisson {len(jobs)} jobs over {args.serve_seconds:.0f} s "
+                       f"({len(jobs) / args.serve_seconds:.0f} jobs/s; 70% grid, 30% Henry "
+                       f"1e6-1e7 insertions; {len(fws)} frameworks; config 5)",
+           "hbm_budget_gib": args.serve_budget_gib}
+    for name, slots in (("served", 8), ("plain", 1)):
+        with serve.Server(ctx, int(args.serve_budget_gib * (1 << 30)), slots) as srv:
+            # atom arrays resident first (one small Henry job per framework)
+            for k, d in enumerate(descs):
+                srv.wait(srv.submit_henry(k, d, 298.0, 1000, 0))
+            t0 = time.perf_counter()
+            sts = serve.run_stream(srv, schedule())
+            wall = time.perf_counter() - t0
+        lat = np.array([st["latency_s"] for st in sts], dtype=np.float64) * 1e3
+        kinds = np.array([j["kind"] for j in jobs])
+        res[name] = {"slots": slots, "p50_ms": float(np.percentile(lat, 50)),
+                     "p99_ms": float(np.percentile(lat, 99)),
+                     "grid_p50_ms": float(np.percentile(lat[kinds == "grid"], 50)),
+                     "henry_p50_ms": float(np.percentile(lat[kinds == "henry"], 50)),
+                     "jobs_per_s": len(sts) / wall,
+                     "failed": int(sum(1 for st in sts if st["status"] != 0))}
+    return res
 
 
 def load_traffic(pairs_step):
@@ -447,6 +553,12 @@ def main():
     ap.add_argument("--dims", type=int, default=256)
     ap.add_argument("--insertions", type=int, default=10_000_000)
     ap.add_argument("--tile", type=int, default=4, choices=[4, 8])
+    ap.add_argument("--no-widom", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--widom-frameworks", type=int, default=64)
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the Poisson stream (the full config-5 stream is 60 s)")
+    ap.add_argument("--serve-budget-gib", type=float, default=48.0)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.case != "batch":

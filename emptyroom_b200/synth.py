@@ -118,3 +118,52 @@ def config3(seed=3):
     return make_framework(seed, (30.1, 32.4, 28.7), (85.0, 95.0, 110.0), 4096, n_types=4,
                           probe="CH4", rc=12.5, d_min=1.2, dims=(256, 256, 256),
                           name="config3")
+
+
+def config4(n_frameworks=64, seed=4000, spacing=0.2):
+    """Widom batch: 64 config-1 cells (cubic 25.8 A, 424 atoms, d_min 1.2 A, 4
+    types), Xe probe, pocket-blocking grid at 0.2 A (130^3)."""
+    abc = (25.8, 25.8, 25.8)
+    dims = grid_dims_for(abc, spacing)
+    return [make_framework(seed + k, abc, (90.0, 90.0, 90.0), 424, n_types=4, probe="Xe",
+                           rc=12.5, d_min=1.2, dims=dims, name=f"config4_{k}")
+            for k in range(n_frameworks)]
+
+
+def config5_stream(seed=5000, rate=200.0, seconds=60.0, n_frameworks=32, grid_fraction=0.7,
+                   atoms=(50, 10000), insertions=(1_000_000, 10_000_000),
+                   spacing_range=(0.1, 0.2), max_density=MAX_DENSITY):
+    """Serving stream: Poisson arrivals at `rate` jobs/s for `seconds`; 70 %
+    grid jobs (spacing ~ U[0.1, 0.2] A), 30 % Henry jobs (insertions
+    log-uniform in [1e6, 1e7]); a pool of frameworks with the config-1 cell
+    (cubic 25.8 A), 4 types, atom counts log-uniform in [50, 10000] capped at
+    max_density * V, probes uniform over CH4 / Xe / Kr.
+    Returns (frameworks, jobs); a job is a dict with t (arrival, s), kind
+    ("grid" | "henry"), fw (pool index), dims or n_ins, seed."""
+    rng = np.random.default_rng(seed)
+    abc = (25.8, 25.8, 25.8)
+    t_, _, vol = cell_matrices(*abc, 90.0, 90.0, 90.0)
+    probes = list(PROBES)
+    fws = []
+    for k in range(n_frameworks):
+        n = int(round(math.exp(rng.uniform(math.log(atoms[0]), math.log(atoms[1])))))
+        n = max(1, min(n, int(max_density * vol)))
+        fws.append(make_framework(seed + 1 + k, abc, (90.0, 90.0, 90.0), n, n_types=4,
+                                  probe=probes[int(rng.integers(0, 3))], rc=12.5, d_min=1.2,
+                                  name=f"config5_{k}"))
+    jobs = []
+    t = 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= seconds:
+            break
+        fw = int(rng.integers(0, n_frameworks))
+        if rng.random() < grid_fraction:
+            dims = grid_dims_for(abc, float(rng.uniform(*spacing_range)))
+            jobs.append({"t": t, "kind": "grid", "fw": fw, "dims": dims})
+        else:
+            n_ins = int(round(math.exp(rng.uniform(math.log(insertions[0]),
+                                                   math.log(insertions[1])))))
+            jobs.append({"t": t, "kind": "henry", "fw": fw, "n_ins": n_ins,
+                         "seed": int(rng.integers(0, 2**31))})
+    return fws, jobs
