@@ -32,6 +32,7 @@ ER_BATCH_PLAIN = 1
 ER_BATCH_HOST_OUT = 0x100
 ER_BATCH_AUTOTUNE = 0x200
 ER_ENERGY_CAP = 1.0e30
+ER_INTERP_GRID_F64 = 0x1
 R_GAS = 8.314  # J/(mol K), src/henry.cu:169
 
 
@@ -322,6 +323,18 @@ class Context:
             return g, n.value, seg
         return g, n.value
 
+    def grid_interp(self, grid_ptr, dims, pts, f64=False):
+        """GCMC guest-framework energies at fractional points (n, 3) by trilinear
+        lookup in a device grid (float, or double with f64=True); host in/out."""
+        q = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(len(q), dtype=np.float64)
+        _grid_interp(self, grid_ptr, dims, q.ctypes.data, len(q), out.ctypes.data, f64)
+        return out
+
+    def grid_interp_device(self, grid_ptr, dims, pts_ptr, n, out_ptr, f64=False):
+        """As grid_interp with points and results in device memory."""
+        _grid_interp(self, grid_ptr, dims, pts_ptr, n, out_ptr, f64)
+
     def block_pockets_device(self, grid_ptr, dims, temperature, mask_ptr):
         nx, ny, nz = (int(x) for x in dims)
         n = ctypes.c_int(0)
@@ -329,6 +342,14 @@ class Context:
             self._h, ctypes.c_void_p(int(grid_ptr)), nx, ny, nz, float(temperature),
             ctypes.c_void_p(int(mask_ptr)), ctypes.byref(n)))
         return n.value
+
+
+def _grid_interp(ctx, grid_ptr, dims, pts_ptr, n, out_ptr, f64):
+    nx, ny, nz = (int(x) for x in dims)
+    ctx._check(_capi.lib().er_grid_interp(
+        ctx._h, ctypes.c_void_p(int(grid_ptr)), nx, ny, nz, ER_INTERP_GRID_F64 if f64 else 0,
+        ctypes.cast(ctypes.c_void_p(int(pts_ptr)), ctypes.POINTER(ctypes.c_double)), int(n),
+        ctypes.cast(ctypes.c_void_p(int(out_ptr)), ctypes.POINTER(ctypes.c_double))))
 
 
 class BatchPlan:

@@ -91,6 +91,8 @@ SIGNATURES = {
     "er_block_pockets": (c_int, [c_void_p, _dp, c_int, c_int, c_int, c_double, _ip, _ip]),
     "er_block_pockets_device": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_double,
                                         c_void_p, _ip]),
+    "er_grid_interp": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, _dp, c_int64,
+                               _dp]),
     "er_cell_matrices": (c_int, [c_double, c_double, c_double, c_double, c_double, c_double,
                                  _dp, _dp, _dp]),
     "er_replication_factors": (c_int, [_dp, c_double, c_int, _ip]),

@@ -402,7 +402,7 @@ void er_ctx_destroy(er_ctx* ctx) {
     ctx->fws.clear();
     DevBuf* bufs[] = {&ctx->grid_f32, &ctx->counter,
                       &ctx->p_grid,   &ctx->p_lab,  &ctx->p_seg,  &ctx->p_flags,
-                      &ctx->p_misc,   &ctx->p_mask, &ctx->sheet_cache.grid};
+                      &ctx->p_misc,   &ctx->p_mask, &ctx->sheet_cache.grid, &ctx->interp};
     for (DevBuf* b : bufs) b->release();
     ctx->henry.release();
     ctx->pinned.release();

@@ -87,6 +87,8 @@ struct er_ctx {
     er::HenryScratch henry;
     // pocket-blocking scratch
     er::DevBuf p_grid, p_lab, p_seg, p_flags, p_misc, p_mask;
+    // staging of host points / results for er_grid_interp
+    er::DevBuf interp;
     // device-resident grid cache for er_grid_sheet: key (fw, nx, ny, nz)
     struct SheetCache {
         int fw = 0, nx = 0, ny = 0, nz = 0;

@@ -211,6 +211,20 @@ int er_block_pockets(er_ctx* ctx, double* grid, int nx, int ny, int nz, double t
 int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, int ny, int nz,
                             double temperature, uint8_t* pocket_mask_out, int* n_pockets);
 
+/* ------------------------------------------------------------------ GCMC lookup */
+/* Guest-framework energies of a GCMC code by trilinear interpolation of a
+ * device-resident grid: out[q] = GuestFrameworkEnergy(WrapToInterval(x, 1),
+ * WrapToInterval(y, 1), WrapToInterval(z, 1)) of src/gcmc.cc:145-177 and
+ * :74-77 at pts[3q..3q+2] (fractional), FP64 arithmetic in the reference's
+ * order, so equal bit for bit to the reference function on the same grid
+ * values. grid: device memory, nx*ny*nz, layout k + j nz + i ny nz, float
+ * (as er_grid writes it) or double with ER_INTERP_GRID_F64. pts / out: host
+ * or device memory. The lower corner index is clamped to N - 2 (the reference
+ * reads past the grid when x / dx rounds up to N - 1 for x just below 1). */
+#define ER_INTERP_GRID_F64 0x1
+int er_grid_interp(er_ctx* ctx, const void* grid, int nx, int ny, int nz, int flags,
+                   const double* pts, int64_t n, double* out);
+
 /* ------------------------------------------------------------------ host helpers */
 /* Fractional -> Cartesian matrix and its inverse from cell lengths (A) and
  * angles (degrees), the formulas of src/Framework.cc:113-142. Returns

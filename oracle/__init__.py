@@ -72,6 +72,9 @@ def lib():
         L.oracle_block_pockets.restype = ctypes.c_int
         L.oracle_block_pockets.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, _ip]
+        L.oracle_grid_interp.restype = None
+        L.oracle_grid_interp.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                         ctypes.c_int64, _dp]
         _lib = L
     return _lib
 
@@ -104,6 +107,10 @@ def ref():
         R.ref_load_framework.restype = ctypes.c_int
         R.ref_load_framework.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _dp, _dp,
                                          ctypes.c_int]
+        if hasattr(R, "ref_grid_interp"):
+            R.ref_grid_interp.restype = None
+            R.ref_grid_interp.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
+                                          ctypes.c_int64, _dp]
         R.ref_load_forcefield.restype = ctypes.c_int
         R.ref_load_forcefield.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _dp, _dp,
                                           ctypes.c_int]
@@ -300,3 +307,28 @@ def ref_load_forcefield(root, name, max_entries=10000):
     n = R.ref_load_forcefield(str(root).encode(), name.encode(), _ptr(eps, _dp),
                               _ptr(sig, _dp), max_entries)
     return eps[:n].copy(), sig[:n].copy()
+
+
+def grid_interp(grid, pts):
+    """GCMC trilinear lookup (src/gcmc.cc:145-177 at WrapToInterval(., 1)),
+    restated; grid (nx, ny, nz) float64, pts (n, 3) fractional."""
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    q = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(len(q), dtype=np.float64)
+    nx, ny, nz = g.shape
+    lib().oracle_grid_interp(_ptr(g, _dp), nx, ny, nz, _ptr(q, _dp), len(q), _ptr(out, _dp))
+    return out
+
+
+def ref_grid_interp(grid, pts):
+    """The reference's own GuestFrameworkEnergy / WrapToInterval (extracted from
+    src/gcmc.cc at build time) on the same inputs."""
+    R = ref()
+    if R is None or not hasattr(R, "ref_grid_interp"):
+        raise RuntimeError("oracle/_ref/libref.so not built with the GCMC lookup")
+    g = np.array(grid, dtype=np.float64, order="C", copy=True)
+    q = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(len(q), dtype=np.float64)
+    nx, ny, nz = g.shape
+    R.ref_grid_interp(_ptr(g, _dp), nx, ny, nz, _ptr(q, _dp), len(q), _ptr(out, _dp))
+    return out

@@ -562,3 +562,32 @@ int oracle_block_pockets(double* grid, int nx, int ny, int nz, double temperatur
     free(seg);
     return n_pockets;
 }
+
+/* ------------------------------------------------------------------------
+ * GCMC trilinear lookup, src/gcmc.cc:74-77 and :137-177 (see er_oracle.h). */
+static double gi_wrap1(double x) { return x - 1.0 * floor(x / 1.0); }
+
+void oracle_grid_interp(const double* grid, int nx, int ny, int nz, const double* pts,
+                        int64_t n, double* out) {
+    const double dx = 1.0 / (nx - 1), dy = 1.0 / (ny - 1), dz = 1.0 / (nz - 1);
+    for (int64_t q = 0; q < n; ++q) {
+        const double x = gi_wrap1(pts[3 * q]), y = gi_wrap1(pts[3 * q + 1]),
+                     z = gi_wrap1(pts[3 * q + 2]);
+        int i = (int)floor(x / dx), j = (int)floor(y / dy), k = (int)floor(z / dz);
+        if (i > nx - 2) i = nx - 2;
+        if (j > ny - 2) j = ny - 2;
+        if (k > nz - 2) k = nz - 2;
+        const double xd = (x - i * dx) / dx;
+        const double yd = (y - j * dy) / dy;
+        const double zd = (z - k * dz) / dz;
+#define G(a, b, c) grid[(size_t)(c) + (size_t)(b) * nz + (size_t)(a) * ny * nz]
+        const double c00 = G(i, j, k) * (1.0 - xd) + xd * G(i + 1, j, k);
+        const double c10 = G(i, j + 1, k) * (1.0 - xd) + xd * G(i + 1, j + 1, k);
+        const double c01 = G(i, j, k + 1) * (1.0 - xd) + xd * G(i + 1, j, k + 1);
+        const double c11 = G(i, j + 1, k + 1) * (1.0 - xd) + xd * G(i + 1, j + 1, k + 1);
+#undef G
+        const double c0 = c00 * (1.0 - yd) + c10 * yd;
+        const double c1 = c01 * (1.0 - yd) + c11 * yd;
+        out[q] = c0 * (1.0 - zd) + c1 * zd;
+    }
+}

@@ -101,6 +101,15 @@ void oracle_henry(const or_particle* atoms, int n_atoms, const double t[9], cons
 int oracle_block_pockets(double* grid, int nx, int ny, int nz, double temperature,
                          int* segment_out);
 
+/* GCMC guest-framework energy by trilinear interpolation of a grid,
+ * src/gcmc.cc:145-177, at WrapToInterval(x, 1) of each coordinate
+ * (src/gcmc.cc:74-77, applied at the call sites :191-194); grid spacing
+ * 1 / (N - 1) (src/gcmc.cc:343), layout k + j nz + i ny nz. The lower corner
+ * index is clamped to N - 2 (the reference reads past the grid when x / dx
+ * rounds up to N - 1 for x just below 1). */
+void oracle_grid_interp(const double* grid, int nx, int ny, int nz, const double* pts,
+                        int64_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,7 +7,8 @@ built from it by `make -C oracle`):
 
 Each fixture stores seeded inputs and the outputs that the reference's code
 (src/computegridsheet.h kernels compiled as host C++, src/pocketblocking.cc,
-src/Framework.cc, src/Forcefield.cc) produced for them, so tests can pin the
+src/Framework.cc, src/Forcefield.cc, the grid lookup of src/gcmc.cc) produced
+for them, so tests can pin the
 oracle restatement and the CUDA path on machines without the reference.
 """
 from __future__ import annotations
@@ -112,6 +113,16 @@ def main():
         E = percolation_grid(seed, dims, T, p)
         blocked, n = oracle.ref_block_pockets(E, T)
         out[key] = dict(grid=E, T=np.float64(T), blocked=blocked, n_pockets=np.int32(n))
+    # GCMC lookup: a config-1 grid with two blocked pockets, points inside and
+    # outside [0, 1) (the call sites wrap them)
+    g1 = out["grid_cubic"]["grid"].copy()
+    g1[2, 3, 4] = 1e13
+    g1[6, 7, 8] = 1e13
+    rng = np.random.default_rng(26)
+    pts = np.concatenate([rng.uniform(0.0, 1.0, size=(400, 3)),
+                          rng.uniform(-2.0, 3.0, size=(200, 3)),
+                          np.array([[0.0, 0.0, 0.0], [0.5, 0.5, 0.5], [0.125, 0.25, 0.375]])])
+    out["gcmc_interp"] = dict(grid=g1, pts=pts, energy=oracle.ref_grid_interp(g1, pts))
     # loaders on a fixture tree written in the reference's formats
     with tempfile.TemporaryDirectory() as tmp:
         write_fixture_tree(tmp)

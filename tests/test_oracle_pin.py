@@ -96,3 +96,21 @@ def test_oracle_pockets_match_reference_live(seed, p):
     b1, n1, _ = oracle.block_pockets(E, T)
     b2, n2 = oracle.ref_block_pockets(E, T)
     assert n1 == n2 and np.array_equal(b1, b2)
+
+
+def test_oracle_interp_matches_golden_bitwise():
+    """GCMC lookup restatement vs the reference's GuestFrameworkEnergy
+    (src/gcmc.cc:145-177) on the golden grid and points."""
+    g = golden("gcmc_interp")
+    assert np.array_equal(oracle.grid_interp(g["grid"], g["pts"]), g["energy"])
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference not built here")
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_interp_matches_reference_live(seed):
+    rng = np.random.default_rng(seed)
+    dims = tuple(int(x) for x in rng.integers(2, 30, size=3))
+    grid = rng.normal(size=dims) * 100.0
+    grid[rng.random(dims) < 0.05] = 1e13
+    pts = rng.uniform(-3.0, 4.0, size=(3000, 3))
+    assert np.array_equal(oracle.grid_interp(grid, pts), oracle.ref_grid_interp(grid, pts))
