@@ -126,9 +126,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(rank):
+def make_workload(rank, n=256):
     from emptyroom_b200 import synth
-    return synth.config2(n_frameworks=256, seed=1000 + 100000 * rank)
+    return synth.config2(n_frameworks=n, seed=1000 + 100000 * rank)
 
 
 def upload_all(ctx, fws):
@@ -215,7 +215,7 @@ def run_ours(args, ws, rank, local, pg):
     import emptyroom_b200 as er
     torch.cuda.set_device(local)
     ctx = er.Context(local)
-    fws = make_workload(rank)
+    fws = make_workload(rank, args.frameworks)
     ups = upload_all(ctx, fws)
     counts = count_pairs(ctx, ups, fws)
     pairs_step = float(sum(counts))
@@ -285,13 +285,14 @@ def run_ours(args, ws, rank, local, pg):
     roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fp32_rate / 1e12,
             "unit": "Tinst/s", "frac": achieved / fp32_rate,
             "peak_source": "measured FP32 FFMA issue rate (er_probe_fp32_rate) on this GPU",
-            "traffic": load_traffic(pairs_step)}
+            "traffic": load_traffic(points_step)}
     line = {
         "metric": METRIC, "value": value, "unit": "pair-terms/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic (seeded frameworks; no dataset ships with the reference)",
-        "config": {"workload": "256-framework batched LJ grids (config 2)", "frameworks": 256,
+        "config": {"workload": f"{len(fws)}-framework batched LJ grids (config 2)",
+                   "frameworks": len(fws),
                    "grid_points_per_step": int(points_step), "pair_terms_per_step": int(pairs_step),
                    "cutoff_A": 12.5, "spacing_A": [0.1, 0.2],
                    "l2": "flushed between timed steps (256 MB write)",
@@ -427,14 +428,15 @@ def run_serving(ctx, args):
     return res
 
 
-def load_traffic(pairs_step):
+def load_traffic(points_step):
     """DRAM bytes per launch of the persistent kernel from the committed ncu
-    summary (profiles/grid_persistent_traffic.json), scaled by pair terms."""
+    capture of a smaller batch (profiles/grid_persistent_traffic.json), scaled
+    to this launch by grid points (the traffic is the grid store)."""
     p = os.path.join(ROOT, "profiles", "grid_persistent_traffic.json")
     if not os.path.exists(p):
         return None
     d = json.load(open(p))
-    return d["dram_bytes_per_pair"] * pairs_step
+    return d["dram_bytes_per_point"] * points_step
 
 
 def run_reference(args, ws, rank):
@@ -553,6 +555,8 @@ def main():
     ap.add_argument("--dims", type=int, default=256)
     ap.add_argument("--insertions", type=int, default=10_000_000)
     ap.add_argument("--tile", type=int, default=4, choices=[4, 8])
+    ap.add_argument("--frameworks", type=int, default=256,
+                    help="frameworks of the batch (256 is the workload; fewer for profiling)")
     ap.add_argument("--no-widom", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--widom-frameworks", type=int, default=64)
