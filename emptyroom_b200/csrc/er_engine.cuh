@@ -291,7 +291,8 @@ struct GridPolicy {
 };
 
 // Widom insertion points: CTA c owns sorted positions [256 P c, 256 P (c + 1))
-// of `order`; warp w the 32 P positions from 256 P c + 32 P w.
+// of `order` (points stored in that order); warp w the 32 P positions from
+// 256 P c + 32 P w, lane l position p * 32 + l of them.
 template <int P_>
 struct PointPolicy {
     static constexpr int kP = P_;
@@ -305,12 +306,12 @@ struct PointPolicy {
         return pos < nv ? T->order[pos] : -1;
     }
     __device__ __forceinline__ bool point(int w, int lane, int p, double* f) const {
-        int idx = slot_index(w, lane, p);
-        const bool ok = idx >= 0;
-        if (!ok) idx = T->order[min(base, nv - 1)];  // a finite stand-in, never stored
-        f[0] = T->pts[3 * (size_t)idx];
-        f[1] = T->pts[3 * (size_t)idx + 1];
-        f[2] = T->pts[3 * (size_t)idx + 2];
+        int pos = base + w * (32 * kP) + p * 32 + lane;
+        const bool ok = pos < nv;
+        if (!ok) pos = min(base, nv - 1);  // a finite stand-in, never stored
+        f[0] = T->pts[3 * (size_t)pos];
+        f[1] = T->pts[3 * (size_t)pos + 1];
+        f[2] = T->pts[3 * (size_t)pos + 2];
         return ok;
     }
     __device__ __forceinline__ void store(int w, int lane, int p, float e) const {
@@ -494,6 +495,100 @@ __device__ __forceinline__ int lattice_shell(EngineSmem& s, const unsigned short
             atom(wl[kMaxCand - 1 - q], q);
             ++q;
         }
+        if (kComp) fold_packed<M>(s, acc2);
+    }
+    if (!kComp) fold_packed<M>(s, acc2);
+    return nrec;
+}
+
+// Generic (per-point x, y, z) inner and shell lists, packed over point pairs
+// (2m, 2m + 1): per two pair terms 9 packed FP32x2 instructions and 2
+// MUFU.RCP; r^2 = fma(dz, dz, fma(dy, dy, dx * dx)) as in r2_generic, so the
+// borderline re-check reproduces it bit for bit.
+template <class Pol, int PREC>
+__device__ __forceinline__ int generic_packed_lists(EngineSmem& s, const unsigned short* wl,
+                                                    int n_in, int n_sh, float rc2f, float win,
+                                                    Lane<Pol, PREC>& L, unsigned& rec) {
+    constexpr int M = Pol::kP / 2;
+    constexpr bool kComp = PrecTraits<PREC>::comp;
+    f2_t px2[M], py2[M], pz2[M], acc2[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        px2[m] = f2_pack(L.px[2 * m], L.px[2 * m + 1]);
+        py2[m] = f2_pack(L.py[2 * m], L.py[2 * m + 1]);
+        pz2[m] = f2_pack(L.pz[2 * m], L.pz[2 * m + 1]);
+        acc2[m] = 0ull;
+    }
+    const f2_t one2 = f2_pack(1.0f, 1.0f);
+    const f2_t rc2 = f2_pack(rc2f, rc2f);
+    const char* cbase = reinterpret_cast<const char*>(s.cand);
+    int nrec = 0;
+    rec = 0;
+    auto inner_atom = [&](unsigned off) {
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);       // x x | y z
+        const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(cbase + off + 16);  // C12 | -C6
+        if (PREC == PREC_COUNT) {
+#pragma unroll
+            for (int m = 0; m < M; ++m) acc2[m] = f2_add(acc2[m], one2);
+            return;
+        }
+        float ay, az;
+        f2_unpack(v0.y, ay, az);
+        const f2_t ay2 = f2_pack(ay, ay), az2 = f2_pack(az, az);
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const f2_t dx = f2_sub(px2[m], v0.x);
+            const f2_t dy = f2_sub(py2[m], ay2);
+            const f2_t dz = f2_sub(pz2[m], az2);
+            const f2_t r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            float r0, r1;
+            f2_unpack(r2, r0, r1);
+            const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
+            const f2_t u3 = f2_mul(f2_mul(u, u), u);
+            acc2[m] = f2_fma(u3, f2_fma(v1.x, u3, v1.y), acc2[m]);
+        }
+    };
+    auto shell_atom = [&](unsigned off, int q) {
+        const ulonglong2 v0 = *reinterpret_cast<const ulonglong2*>(cbase + off);
+        const ulonglong2 v1 = *reinterpret_cast<const ulonglong2*>(cbase + off + 16);
+        float ay, az;
+        f2_unpack(v0.y, ay, az);
+        const f2_t ay2 = f2_pack(ay, ay), az2 = f2_pack(az, az);
+        float mn = INFINITY;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+            const f2_t dx = f2_sub(px2[m], v0.x);
+            const f2_t dy = f2_sub(py2[m], ay2);
+            const f2_t dz = f2_sub(pz2[m], az2);
+            const f2_t r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+            float r0, r1, d0, d1;
+            f2_unpack(r2, r0, r1);
+            const f2_t in = f2_pack(set_lt(r0, rc2f), set_lt(r1, rc2f));
+            f2_unpack(f2_sub(r2, rc2), d0, d1);
+            mn = fminf(mn, fminf(fabsf(d0), fabsf(d1)));
+            if (PREC == PREC_COUNT) {
+                acc2[m] = f2_add(acc2[m], in);
+            } else {
+                const f2_t u = f2_pack(rcp_approx(r0), rcp_approx(r1));
+                const f2_t u3 = f2_mul(f2_mul(u, u), u);
+                acc2[m] = f2_fma(f2_mul(u3, in), f2_fma(v1.x, u3, v1.y), acc2[m]);
+            }
+        }
+        if (mn <= win) {  // rare: a pair of this atom sits near the cutoff
+            rec = (rec << 10) | (unsigned)q;
+            ++nrec;
+        }
+    };
+    int q = 0;
+    while (q < n_in) {
+        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
+        for (; q < qe; ++q) inner_atom(wl[q]);
+        if (kComp) fold_packed<M>(s, acc2);
+    }
+    q = 0;
+    while (q < n_sh) {
+        const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
+        for (; q < qe; ++q) shell_atom(wl[kMaxCand - 1 - q], q);
         if (kComp) fold_packed<M>(s, acc2);
     }
     if (!kComp) fold_packed<M>(s, acc2);
@@ -741,7 +836,9 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         lattice_inner<Pol, PREC>(s, wl, n_in, L);
         nrec = lattice_shell<Pol, PREC>(s, wl, n_sh, rc2f, win, L, rec);
     } else {
-        nrec = generic_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, rec);
+        nrec = (Pol::kP % 2 == 0)
+                   ? generic_packed_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, rec)
+                   : generic_lists<Pol, PREC>(s, wl, n_in, n_sh, rc2f, win, L, rec);
     }
 
     // --- exact re-decision of borderline shell pairs (rare); lanes without a
@@ -749,6 +846,7 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
     if (nrec > 0) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, nrec, rec, L);
     // --- near list in FP64: exact positions (FP64 images and points relative
     // to the CTA centre) and FP64 (C12, C6); all near atoms are inner atoms.
+    // Atom-outer order: one atom's loads serve the lane's P points.
     if (kNear && n_near > 0) {
         double qx[P], qy[P], qz[P], o0, o1, o2;
         cta_centre(s, o0, o1, o2);

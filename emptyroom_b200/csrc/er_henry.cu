@@ -3,11 +3,11 @@
 // Replaces doHenry (src/doHenry.h:29-135) and its host reduction
 // (src/henry.cu:157-174). Pipeline, all on the context stream:
 //   1. gen     insertion i -> Philox4x32-10 point (stream `seed`), pocket-mask
-//              test, spatial bin key (bins of ~16 expected points, 2x2x2 bricks)
+//              test, spatial bin key (bins of ~32 expected points, 2x2x2 bricks)
 //   2. scan    bin counts -> bin starts
 //   3. scatter insertion indices into their bins; 4. sort each bin ascending
 //      (so the layout, and with it every FP32 rounding, is deterministic)
-//   5. energy  the shared LJ engine over 1024 sorted points per CTA
+//   5. energy  the shared LJ engine over 2048 sorted points per CTA
 //   6. reduce  FP64 log-sum-exp of exp(-E/T) and E exp(-E/T) in insertion
 //              order with a fixed tree: (m, s, se) with sum w = s e^m.
 #include <math.h>
@@ -20,7 +20,7 @@
 
 namespace er {
 
-constexpr int kHenryP = 4;  // insertions per thread of the energy kernel
+constexpr int kHenryP = 8;  // insertions per thread of the energy kernel
 
 struct BinGeom {
     int nb[3];  // bins per fractional axis
@@ -60,15 +60,12 @@ __device__ __forceinline__ bool blocked_at(const uint8_t* mask, int nx, int ny, 
 }
 
 __global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t* __restrict__ mask,
-                                 int mnx, int mny, int mnz, double* __restrict__ pts,
-                                 int* __restrict__ key, int* __restrict__ counts,
-                                 float* __restrict__ energies, int* __restrict__ n_blocked) {
+                                 int mnx, int mny, int mnz, int* __restrict__ key,
+                                 int* __restrict__ counts, float* __restrict__ energies,
+                                 int* __restrict__ n_blocked) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double f[3];
         insertion_point(seed, (uint64_t)i, f);
-        pts[3 * (size_t)i] = f[0];
-        pts[3 * (size_t)i + 1] = f[1];
-        pts[3 * (size_t)i + 2] = f[2];
         if (mask && blocked_at(mask, mnx, mny, mnz, f)) {
             key[i] = -1;
             energies[i] = INFINITY;
@@ -81,31 +78,110 @@ __global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t*
     }
 }
 
-// Exclusive scan of n ints by one CTA of 1024 threads (contiguous chunks);
-// out[n] receives the total.
-__global__ void __launch_bounds__(1024) scan_kernel(const int* __restrict__ in,
-                                                    int* __restrict__ out, int n) {
-    __shared__ int sums[1024];
+// Exclusive scan of n ints (the bin counts) in three coalesced passes over
+// tiles of kScanTile: tile sums, a one-CTA scan of the tile sums, then each
+// tile scanned on chip and offset; out[n] receives the total.
+constexpr int kScanThreads = 256, kScanPer = 8, kScanTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int cta_exscan256(int v, int* wsum, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < kScanThreads / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < kScanThreads / 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < kScanThreads / 32) wsum[lane] = t;
+    }
+    __syncthreads();
+    const int base = w ? wsum[w - 1] : 0;
+    *total = wsum[kScanThreads / 32 - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const int* __restrict__ in,
+                                                                  int n, int* __restrict__ sums) {
+    __shared__ int wsum[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k * kScanThreads + threadIdx.x;
+        if (i < n) v += in[i];
+    }
+    int tot;
+    cta_exscan256(v, wsum, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) scan_top_kernel(int* __restrict__ sums, int n_tiles,
+                                                        int* __restrict__ total_out) {
+    __shared__ int part[1024];
     const int t = threadIdx.x;
-    const int per = (n + 1023) / 1024;
-    const int lo = min(n, t * per), hi = min(n, lo + per);
+    const int per = (n_tiles + 1023) / 1024;  // a few contiguous tile sums per thread
+    const int lo = min(n_tiles, t * per), hi = min(n_tiles, lo + per);
     int s = 0;
-    for (int i = lo; i < hi; ++i) s += in[i];
-    sums[t] = s;
+    for (int i = lo; i < hi; ++i) s += sums[i];
+    part[t] = s;
     __syncthreads();
     for (int o = 1; o < 1024; o <<= 1) {
-        const int v = t >= o ? sums[t - o] : 0;
+        const int v = t >= o ? part[t - o] : 0;
         __syncthreads();
-        sums[t] += v;
+        part[t] += v;
         __syncthreads();
     }
-    int run = sums[t] - s;
+    int run = part[t] - s;
     for (int i = lo; i < hi; ++i) {
-        const int v = in[i];
-        out[i] = run;
+        const int v = sums[i];
+        sums[i] = run;
         run += v;
     }
-    if (t == 1023) out[n] = sums[1023];
+    if (t == 1023) *total_out = part[1023];
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const int* __restrict__ in,
+                                                                  int n,
+                                                                  const int* __restrict__ sums,
+                                                                  int* __restrict__ out) {
+    __shared__ int tile[kScanTile];
+    __shared__ int wsum[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k * kScanThreads + threadIdx.x;
+        tile[k * kScanThreads + threadIdx.x] = i < n ? in[i] : 0;
+    }
+    __syncthreads();
+    // each thread owns kScanPer consecutive entries of the tile
+    int v[kScanPer], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = tile[threadIdx.x * kScanPer + k];
+        s += v[k];
+    }
+    int tot;
+    int run = cta_exscan256(s, wsum, &tot) + sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        tile[threadIdx.x * kScanPer + k] = run;
+        run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k * kScanThreads + threadIdx.x;
+        if (i < n) out[i] = tile[k * kScanThreads + threadIdx.x];
+    }
 }
 
 __global__ void henry_scatter_kernel(const int* __restrict__ key, int n,
@@ -117,9 +193,12 @@ __global__ void henry_scatter_kernel(const int* __restrict__ key, int n,
     }
 }
 
-// One warp per bin: rank of each entry among its bin's entries -> ascending order.
+// One warp per bin: rank of each entry among its bin's entries -> ascending
+// order; the insertion point itself (recomputed from its Philox counter) is
+// written in the same sorted order, so the energy kernel reads it coalesced.
 __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_keys,
-                                       const int* __restrict__ tmp, int* __restrict__ order) {
+                                       const int* __restrict__ tmp, uint64_t seed,
+                                       int* __restrict__ order, double* __restrict__ pts_sorted) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n_keys; b += warps) {
@@ -129,6 +208,11 @@ __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_key
             int rank = 0;
             for (int r = 0; r < L; ++r) rank += tmp[s + r] < v;
             order[s + rank] = v;
+            double f[3];
+            insertion_point(seed, (uint64_t)v, f);
+            pts_sorted[3 * (size_t)(s + rank)] = f[0];
+            pts_sorted[3 * (size_t)(s + rank) + 1] = f[1];
+            pts_sorted[3 * (size_t)(s + rank) + 2] = f[2];
         }
     }
 }
@@ -203,11 +287,12 @@ __global__ void __launch_bounds__(256) henry_final_kernel(const Lse* __restrict_
 int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, uint64_t seed,
                   const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
                   HenryScratch& hs, HenryOut* host_out) {
-    // bins of ~16 expected points, shaped after the cell vector lengths
+    // bins of ~4 P expected points (a 2x2x2 brick of bins ~ one warp's 32 P
+    // points), shaped after the cell vector lengths
     BinGeom g;
     {
         const double L0 = fw.cell_len[0], L1 = fw.cell_len[1], L2 = fw.cell_len[2];
-        const double scale = cbrt((double)n / 16.0 / (L0 * L1 * L2));
+        const double scale = cbrt((double)n / (4.0 * kHenryP) / (L0 * L1 * L2));
         const double L[3] = {L0, L1, L2};
         int64_t nk = 8;
         for (int d = 0; d < 3; ++d) {
@@ -253,14 +338,21 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
     const int gblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads,
                                                (int64_t)ctx->num_sms * 32);
     henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
-                                                   (double*)hs.pts.ptr, (int*)hs.bin.ptr, counts,
-                                                   E, nblk);
-    scan_kernel<<<1, 1024, 0, st>>>(counts, starts, g.n_keys);
+                                                   (int*)hs.bin.ptr, counts, E, nblk);
+    {
+        const int tiles = (g.n_keys + kScanTile - 1) / kScanTile;
+        int* tsum = fill;  // the fill counters are zeroed after the scan
+        scan_tiles_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum);
+        scan_top_kernel<<<1, 1024, 0, st>>>(tsum, tiles, starts + g.n_keys);
+        scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum, starts);
+        ER_CUDA(ctx, cudaMemsetAsync(fill, 0, (size_t)g.n_keys * sizeof(int), st));
+    }
     henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, n, starts, fill,
                                                        (int*)hs.tmp.ptr);
     henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
-                                                              (const int*)hs.tmp.ptr,
-                                                              (int*)hs.order.ptr);
+                                                              (const int*)hs.tmp.ptr, seed,
+                                                              (int*)hs.order.ptr,
+                                                              (double*)hs.pts.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     PointTask task;
     task.fw = fw.dev;

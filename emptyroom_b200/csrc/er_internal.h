@@ -60,7 +60,7 @@ struct GridTask {
 struct PointTask {
     FwDev fw;
     CutoffConsts cc;
-    const double* pts;       // FP64 fractional points, 3 per insertion (insertion order)
+    const double* pts;       // FP64 fractional points, 3 per entry of `order` (bin order)
     const int* order;        // unblocked insertion indices in bin order
     const int* n_valid;      // device count of entries in `order`
     float* energies;         // E per insertion (insertion order)
