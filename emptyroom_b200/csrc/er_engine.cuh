@@ -196,18 +196,27 @@ static __device__ __noinline__ bool exact_in_cutoff(const FwDev& fw, const doubl
 }
 
 // FP64 pair term of image gid at a point q given relative to the CTA centre o.
-__device__ __forceinline__ double pair64(const FwDev& fw, int gid, double qx, double qy,
-                                         double qz, double o0, double o1, double o2,
-                                         double r2min) {
+// One atom image for FP64 pair terms: position relative to the CTA centre and
+// FP64 (C12, C6).
+struct Atom64 {
+    double x, y, z, c12, c6;
+};
+__device__ __forceinline__ Atom64 atom64(const FwDev& fw, int gid, double o0, double o1,
+                                         double o2) {
     const double4 a = fw.img_xyz[gid];
     const int atom = (int)(fw.img_id[gid] / (uint32_t)fw.imgs_per_atom);
     const double2 lj = fw.atom_lj64[atom];
-    const double dx = qx - (a.x - o0), dy = qy - (a.y - o1), dz = qz - (a.z - o2);
+    return Atom64{a.x - o0, a.y - o1, a.z - o2, lj.x, lj.y};
+}
+// FP64 pair term of atom a at a point q (both relative to the CTA centre).
+__device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, double qz,
+                                         double r2min) {
+    const double dx = qx - a.x, dy = qy - a.y, dz = qz - a.z;
     double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
     r2 = fmax(r2, r2min);
     const double u = __drcp_rn(r2);
     const double u3 = u * u * u;
-    return u3 * fma(lj.x, u3, -lj.y);
+    return u3 * fma(a.c12, u3, -a.c6);
 }
 
 // FP32 r^2 of the generic form (each point has its own x, y, z) and of the
@@ -809,7 +818,7 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
             point64(p, qx, qy, qz);
             double acc = 0.0;
             for (int q = 0; q < n_in; ++q)
-                acc += pair64(fw, s.cid[wl[q] >> 5], qx, qy, qz, o0, o1, o2, cc.r2min);
+                acc += pair64(atom64(fw, s.cid[wl[q] >> 5], o0, o1, o2), qx, qy, qz, cc.r2min);
             double f[3];
             pol.point(w, lane, p, f);
             for (int q = 0; q < n_sh; ++q) {
@@ -825,7 +834,7 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
                 bool inside = dd < 0.f;
                 if (fabsf(dd) <= win) inside = exact_in_cutoff(fw, f, s.cid[off >> 5], cc.r2min);
                 if (inside)
-                    acc += pair64(fw, s.cid[off >> 5], qx, qy, qz, o0, o1, o2, cc.r2min);
+                    acc += pair64(atom64(fw, s.cid[off >> 5], o0, o1, o2), qx, qy, qz, cc.r2min);
             }
             tot_at(s, p) += acc;
         }
@@ -856,10 +865,9 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
 #pragma unroll
         for (int p = 0; p < P; ++p) nacc[p] = 0.0;
         for (int q = 0; q < n_near; ++q) {
-            const int gid = s.cid[wn[q] >> 5];
+            const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
 #pragma unroll
-            for (int p = 0; p < P; ++p)
-                nacc[p] += pair64(fw, gid, qx[p], qy[p], qz[p], o0, o1, o2, cc.r2min);
+            for (int p = 0; p < P; ++p) nacc[p] += pair64(a, qx[p], qy[p], qz[p], cc.r2min);
         }
 #pragma unroll
         for (int p = 0; p < P; ++p) tot_at(s, p) += nacc[p];
