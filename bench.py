@@ -418,9 +418,15 @@ def run_serving(ctx, args):
             sts = serve.run_stream(srv, schedule())
             wall = time.perf_counter() - t0
         lat = np.array([st["latency_s"] for st in sts], dtype=np.float64) * 1e3
+        wait = np.array([st["start_s"] - st["submit_s"] for st in sts]) * 1e3
+        serv = np.array([st["finish_s"] - st["start_s"] for st in sts]) * 1e3
         kinds = np.array([j["kind"] for j in jobs])
         res[name] = {"slots": slots, "p50_ms": float(np.percentile(lat, 50)),
                      "p99_ms": float(np.percentile(lat, 99)),
+                     "queue_wait_p50_ms": float(np.percentile(wait, 50)),
+                     "queue_wait_p99_ms": float(np.percentile(wait, 99)),
+                     "service_p50_ms": float(np.percentile(serv, 50)),
+                     "service_p99_ms": float(np.percentile(serv, 99)),
                      "grid_p50_ms": float(np.percentile(lat[kinds == "grid"], 50)),
                      "henry_p50_ms": float(np.percentile(lat[kinds == "henry"], 50)),
                      "jobs_per_s": len(sts) / wall,

@@ -31,10 +31,33 @@ int DevBuf::ensure(size_t bytes) {
     cap = want;
     return ER_OK;
 }
-void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+int DevBuf::ensure_on(size_t bytes, cudaMemPool_t pool, cudaStream_t st) {
+    if (bytes <= cap && ptr) return ER_OK;
+    if (ptr) {
+        if (owner) cudaFreeAsync(ptr, owner);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     cap = 0;
+    owner = nullptr;
+    size_t want = std::max<size_t>(bytes, 256);
+    if (cudaMallocFromPoolAsync(&ptr, want, pool, st) != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return ER_ERR_NOMEM;
+    }
+    cap = want;
+    owner = st;
+    return ER_OK;
+}
+void DevBuf::release() {
+    if (ptr) {
+        if (owner) cudaFreeAsync(ptr, owner);
+        else cudaFree(ptr);
+    }
+    ptr = nullptr;
+    cap = 0;
+    owner = nullptr;
 }
 int HostBuf::ensure(size_t bytes) {
     if (bytes <= cap && ptr) return ER_OK;
@@ -370,9 +393,13 @@ int er_ctx_create(int device, er_ctx** out) {
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = device;
         uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool
+        // no reuse that would make one stream wait for another's pending free
+        int no_dep = 0;
         if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess ||
             cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep) !=
-                cudaSuccess) {
+                cudaSuccess ||
+            cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolReuseAllowInternalDependencies,
+                                    &no_dep) != cudaSuccess) {
             cudaGetLastError();
             if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
             cudaStreamDestroy(ctx->copy_stream);

@@ -29,7 +29,11 @@ struct FwRecord {
 struct DevBuf {
     void* ptr = nullptr;
     size_t cap = 0;
+    cudaStream_t owner = nullptr;  // stream-ordered buffers: the stream they live on
     int ensure(size_t bytes);
+    // Grows from `pool` in stream order on `st` (the old buffer is freed on
+    // `st` too): no device-wide synchronisation, for buffers one stream uses.
+    int ensure_on(size_t bytes, cudaMemPool_t pool, cudaStream_t st);
     void release();
 };
 

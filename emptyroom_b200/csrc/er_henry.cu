@@ -305,12 +305,19 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         g.n_keys = (int)nk;
     }
     const size_t N = (size_t)n;
-    if (hs.pts.ensure(3 * N * sizeof(double)) || hs.bin.ensure(N * sizeof(int)) ||
-        hs.order.ensure(N * sizeof(int)) || hs.tmp.ensure(N * sizeof(int)) ||
-        hs.counts.ensure(2 * (size_t)g.n_keys * sizeof(int)) ||
-        hs.starts.ensure(((size_t)g.n_keys + 1) * sizeof(int)) ||
-        hs.e.ensure(N * sizeof(float)) || hs.nblk.ensure(4 * sizeof(int)) ||
-        hs.part.ensure(4096 * sizeof(Lse)) || hs.res.ensure(sizeof(Lse)))
+    // scratch grows in stream order from the context's pool (no device-wide
+    // synchronisation while other streams run jobs)
+    cudaMemPool_t pool = ctx->pool;
+    if (hs.pts.ensure_on(3 * N * sizeof(double), pool, st) ||
+        hs.bin.ensure_on(N * sizeof(int), pool, st) ||
+        hs.order.ensure_on(N * sizeof(int), pool, st) ||
+        hs.tmp.ensure_on(N * sizeof(int), pool, st) ||
+        hs.counts.ensure_on(2 * (size_t)g.n_keys * sizeof(int), pool, st) ||
+        hs.starts.ensure_on(((size_t)g.n_keys + 1) * sizeof(int), pool, st) ||
+        hs.e.ensure_on(N * sizeof(float), pool, st) ||
+        hs.nblk.ensure_on(4 * sizeof(int), pool, st) ||
+        hs.part.ensure_on(4096 * sizeof(Lse), pool, st) ||
+        hs.res.ensure_on(sizeof(Lse), pool, st))
         return set_error(ctx, ER_ERR_NOMEM, "henry: device scratch allocation failed");
     const uint8_t* d_mask = nullptr;
     if (block_mask) {
@@ -322,7 +329,8 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
             d_mask = block_mask;  // e.g. the output of er_block_pockets_device
         } else {
             const size_t mb = (size_t)mnx * mny * mnz;
-            if (hs.mask.ensure(mb)) return set_error(ctx, ER_ERR_NOMEM, "henry: mask allocation");
+            if (hs.mask.ensure_on(mb, ctx->pool, st))
+                return set_error(ctx, ER_ERR_NOMEM, "henry: mask allocation");
             ER_CUDA(ctx, cudaMemcpyAsync(hs.mask.ptr, block_mask, mb, cudaMemcpyHostToDevice, st));
             d_mask = (const uint8_t*)hs.mask.ptr;
         }

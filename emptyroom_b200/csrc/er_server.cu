@@ -1,13 +1,27 @@
 // er_server.cu -- request server with continuous batching (er_server_*).
 //
-// One scheduler thread per server. Jobs wait in arrival order; the head job
-// is admitted when a slot (a CUDA stream with its own Widom scratch) is free
-// and its device footprint fits the HBM budget after evicting unpinned cached
-// grids (least recently used first). An admitted job's kernels go onto its
-// slot's stream at once, so the device runs the kernels of every admitted job
-// concurrently and new arrivals join while earlier ones are still running.
-// Completion is detected with one event per slot. Frameworks (the image cell
-// lists) and finished grids stay resident and are reused by later jobs.
+// One scheduler thread per server. A slot is a CUDA stream with its own
+// Widom scratch; an admitted job's kernels go onto its slot's stream at once,
+// so the device runs the kernels of every admitted job concurrently and new
+// arrivals join while earlier ones are still running. Completion is detected
+// with one event per slot. Frameworks (the image cell lists) and finished
+// grids stay resident and are reused by later jobs.
+//
+// Admission. Every job's cost is estimated as points (grid points or
+// insertions) x atom density, proportional to its pair terms. Jobs below a
+// running median of the costs seen are "small". With two or more slots, half
+// the slots are created at the device's highest stream priority and half at
+// the lowest: the block scheduler then dispatches the CTAs of small jobs
+// ahead of those of large ones (shortest-job-first at CTA granularity, with
+// no preemption of running CTAs). The pending queue is scanned in arrival
+// order and the first job with a free slot of its class is admitted (small
+// jobs may use either class, large jobs only low-priority slots), unless the
+// oldest job has waited longer than kAgeS: then nothing overtakes it and it
+// takes any free slot. A job is admitted only when its device footprint fits
+// the HBM budget after evicting unpinned cached grids (least recently used
+// first). One slot is the plain one-job-at-a-time loop. The budget is
+// reserved in the context's memory pool when the server is created.
+#include <math.h>
 #include <stdint.h>
 #include <string.h>
 
@@ -59,7 +73,10 @@ struct Slot {
     er::HenryOut* pinned = nullptr;  // host copy of the Widom reduction
     uint64_t ticket = 0;
     bool busy = false;
+    bool high = false;               // created at the highest stream priority
 };
+
+constexpr double kAgeS = 0.05;       // a job waiting longer is overtaken by none
 
 }  // namespace
 
@@ -78,6 +95,8 @@ struct er_server {
     bool stop = false;
     std::thread thr;
     Clock::time_point t0;
+    double cost_log_ema = 0.0;   // running centre of log(cost)
+    bool cost_seen = false;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
     size_t scratch_bytes() const {
@@ -110,19 +129,79 @@ struct er_server {
         j.st.finish_s = now();
     }
 
-    // Returns true when the head job was admitted or resolved.
+    // Points x atoms per A^3 (proportional to the pair terms of the job).
+    double job_cost(const er_job& job) {
+        double rho = 0.01;
+        auto f = fws.find(job.fw_key);
+        if (f != fws.end()) {
+            const er::FwRecord* r = er::find_fw(ctx, f->second.fw_id);
+            if (r && r->volume > 0) rho = r->n_atoms / r->volume;
+        } else if (job.desc) {
+            const double* t = job.desc->t_matrix;
+            const double v = fabs(t[0] * (t[4] * t[8] - t[5] * t[7]) -
+                                  t[1] * (t[3] * t[8] - t[5] * t[6]) +
+                                  t[2] * (t[3] * t[7] - t[4] * t[6]));
+            if (v > 0) rho = job.desc->n_atoms / v;
+        }
+        const double pts = job.kind == ER_JOB_GRID ? (double)job.nx * job.ny * job.nz
+                                                   : (double)job.n_insertions;
+        return std::max(pts, 1.0) * std::max(rho, 1e-4);
+    }
+
+    // A free slot for a job of the given class (-1: none).
+    int pick_slot(bool small, bool any) const {
+        int low = -1, high = -1;
+        for (size_t i = 0; i < slots.size(); ++i) {
+            if (slots[i].busy) continue;
+            if (slots[i].high) {
+                if (high < 0) high = (int)i;
+            } else if (low < 0) {
+                low = (int)i;
+            }
+        }
+        if (slots.size() == 1 || any) return high >= 0 ? high : low;
+        if (small) return high >= 0 ? high : low;
+        return low;
+    }
+
+    // Admits (or resolves) one pending job; returns whether it did.
     bool admit_one() {
         if (pending.empty()) return false;
-        int free_slot = -1;
-        for (size_t i = 0; i < slots.size(); ++i)
-            if (!slots[i].busy) {
-                free_slot = (int)i;
-                break;
+        const double t_now = now();
+        const bool aged = t_now - jobs[pending.front()].st.submit_s > kAgeS;
+        for (auto it = pending.begin(); it != pending.end(); ++it) {
+            const uint64_t ticket = *it;
+            SrvJob& j = jobs[ticket];
+            const double cost = job_cost(j.job);
+            const double lc = log(cost);
+            if (!cost_seen) {
+                cost_log_ema = lc;
+                cost_seen = true;
             }
-        if (free_slot < 0) return false;
-        const uint64_t ticket = pending.front();
-        SrvJob& j = jobs[ticket];
-        Slot& sl = slots[free_slot];
+            const bool small = lc <= cost_log_ema;
+            const bool head = it == pending.begin();
+            const int slot = pick_slot(small, aged && head);
+            if (slot < 0) {
+                if (aged) return false;  // the aged head job goes first
+                continue;
+            }
+            cost_log_ema += 0.05 * (lc - cost_log_ema);
+            const int r = admit(ticket, j, slot);
+            if (r == kWait) return false;
+            pending.erase(it);
+            if (r == kResolved) cv_done.notify_all();
+            return true;
+        }
+        return false;
+    }
+
+    enum { kStarted = 0, kResolved = 1, kWait = 2 };
+
+    // Starts job `ticket` on slot `slot_i`, or resolves it at once (a resident
+    // grid, an error); kWait when its footprint does not fit while other jobs
+    // run.
+    int admit(uint64_t ticket, SrvJob& j, int slot_i) {
+        Slot& sl = slots[slot_i];
         const er_job& job = j.job;
         ++tick;
         // a grid that is already resident completes at once
@@ -137,27 +216,21 @@ struct er_server {
                     cudaMemcpy(job.grid_out_host, g->second.ptr, g->second.bytes,
                                cudaMemcpyDeviceToHost);
                 finish(j, ER_OK);
-                pending.pop_front();
-                cv_done.notify_all();
-                return true;
+                return kResolved;
             }
         }
         // framework resident?
         auto f = fws.find(job.fw_key);
         if (f == fws.end()) {
             if (!job.desc) {
-                pending.pop_front();
                 finish(j, ER_ERR_NOT_FOUND);
-                cv_done.notify_all();
-                return true;
+                return kResolved;
             }
             int fw_id = 0;
             int st = er_framework_upload(ctx, job.desc, &fw_id);
             if (st != ER_OK) {
-                pending.pop_front();
                 finish(j, st);
-                cv_done.notify_all();
-                return true;
+                return kResolved;
             }
             SrvFw rec;
             rec.fw_id = fw_id;
@@ -179,11 +252,9 @@ struct er_server {
             // nothing left to evict: wait for running jobs, or fail if none run
             bool any_busy = false;
             for (const Slot& s : slots) any_busy |= s.busy;
-            if (any_busy) return false;
-            pending.pop_front();
+            if (any_busy) return kWait;
             finish(j, ER_ERR_NOMEM);
-            cv_done.notify_all();
-            return true;
+            return kResolved;
         }
         f->second.last_use = tick;
         f->second.pins++;
@@ -192,7 +263,8 @@ struct er_server {
         if (job.kind == ER_JOB_GRID) {
             SrvGrid g;
             g.bytes = need;
-            if (cudaMallocAsync((void**)&g.ptr, g.bytes, sl.stream) != cudaSuccess) {
+            if (cudaMallocFromPoolAsync((void**)&g.ptr, g.bytes, ctx->pool, sl.stream) !=
+                cudaSuccess) {
                 cudaGetLastError();
                 st = ER_ERR_NOMEM;
             } else {
@@ -220,18 +292,16 @@ struct er_server {
                 st = er::henry_enqueue(ctx, *fr, job.temperature, (int)job.n_insertions, job.seed,
                                        nullptr, 0, 0, 0, sl.stream, sl.hs, sl.pinned);
         }
-        pending.pop_front();
         if (st != ER_OK) {
             f->second.pins--;
             finish(j, st);
-            cv_done.notify_all();
-            return true;
+            return kResolved;
         }
         cudaEventRecord(sl.done, sl.stream);
         sl.busy = true;
         sl.ticket = ticket;
-        j.slot = free_slot;
-        return true;
+        j.slot = slot_i;
+        return kStarted;
     }
 
     bool reap() {
@@ -291,14 +361,43 @@ int er_server_create(er_ctx* ctx, size_t hbm_budget_bytes, int slots, er_server*
     s->budget = hbm_budget_bytes;
     s->t0 = Clock::now();
     s->slots.resize(slots);
-    for (Slot& sl : s->slots) {
-        if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
+    int prio_least = 0, prio_greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest) != cudaSuccess) {
+        cudaGetLastError();
+        prio_least = prio_greatest = 0;
+    }
+    for (int i = 0; i < slots; ++i) {
+        Slot& sl = s->slots[i];
+        sl.high = slots > 1 && i < slots / 2;
+        const int prio = slots == 1 ? 0 : (sl.high ? prio_greatest : prio_least);
+        if (cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost((void**)&sl.pinned, sizeof(HenryOut)) != cudaSuccess) {
             cudaGetLastError();
             er_server_destroy(s);
             return set_error(ctx, ER_ERR_CUDA, "server: stream/event creation failed");
         }
+    }
+    // Reserve the budget in the context's pool up front (allocate, free: the
+    // pool keeps the memory), so that admissions carve grids and scratch out
+    // of mapped memory instead of growing the pool on the request path.
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            free_b = 0;
+        }
+        size_t want = std::min(hbm_budget_bytes, (size_t)(0.9 * (double)free_b));
+        void* p = nullptr;
+        while (want >= (64u << 20)) {
+            if (cudaMallocFromPoolAsync(&p, want, ctx->pool, ctx->stream) == cudaSuccess) {
+                cudaFreeAsync(p, ctx->stream);
+                break;
+            }
+            cudaGetLastError();
+            want /= 2;
+        }
+        cudaStreamSynchronize(ctx->stream);
     }
     s->thr = std::thread([s]() { s->run(); });
     *out = s;
@@ -388,7 +487,8 @@ void er_server_destroy(er_server* s) {
         if (sl.pinned) cudaFreeHost(sl.pinned);
         if (sl.done) cudaEventDestroy(sl.done);
     }
-    for (auto& kv : s->grids) cudaFree(kv.second.ptr);
+    for (auto& kv : s->grids) cudaFreeAsync(kv.second.ptr, s->ctx->stream);
+    cudaStreamSynchronize(s->ctx->stream);
     for (auto& kv : s->fws) er_framework_release(s->ctx, kv.second.fw_id);
     for (Slot& sl : s->slots)
         if (sl.stream) cudaStreamDestroy(sl.stream);
