@@ -49,7 +49,7 @@ def dist_setup():
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
         pg = dist
     return ws, rank, local, pg
 
