@@ -209,6 +209,22 @@ def cpu_baseline(fws, counts_fn, target_s=12.0):
                       f"({done_pairs:.3g} pair terms in {done_s:.1f} s)"}
 
 
+def cpu_config1_grid():
+    """The reference's ComputeGridSheet on the whole config-1 32^3 grid, all
+    host cores (seconds)."""
+    import oracle
+    from emptyroom_b200 import synth
+    f = synth.config1(0)
+    P = f.particles()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    if oracle.ref_available():
+        oracle.ref_grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
+    else:
+        oracle.grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
+    return time.perf_counter() - t0
+
+
 def run_ours(args, ws, rank, local, pg):
     import torch
 
@@ -309,6 +325,8 @@ def run_ours(args, ws, rank, local, pg):
     }
     # the Widom and serving forms of the metric, at N = 1 (the batch above is
     # the scaled workload)
+    if ws == 1:
+        line["config1"] = run_config1(ctx)
     if ws == 1 and not args.no_widom:
         line["widom"] = run_widom(ctx, args)
     if ws == 1 and not args.no_serving:
@@ -324,6 +342,7 @@ def run_ours(args, ws, rank, local, pg):
             return float(c[i].astype(np.float64).sum())
 
         line["cpu_baseline"] = cpu_baseline(fws, sheet_pairs)
+        line["cpu_baseline"]["config1_grid_s"] = cpu_config1_grid()
     ctx.close()
     return line
 
@@ -383,6 +402,32 @@ def run_widom(ctx, args):
             "n_pockets_total": int(sum(r[0] for r in res)),
             "n_blocked_total": int(sum(r[1]["n_blocked"] for r in res)),
             "kh_mol_m3_pa_first": res[0][1]["kh_mol_m3_pa"]}
+
+
+def run_config1(ctx):
+    """Config 1 as specified: the cubic 25.8 A cell (424 atoms, CH4), its 32^3
+    FP64 energy grid and 1e5 Widom insertions at 298 K, each through the C
+    ABI with host output (upload included), wall-clocked, best of 5."""
+    from emptyroom_b200 import synth
+    f = synth.config1(0)
+    P = f.particles()
+    res = {"workload": "config-1 cell: 32^3 FP64 grid to host + 1e5 Widom insertions, 298 K"}
+    tg, th = [], []
+    for k in range(6):
+        t0 = time.perf_counter()
+        fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+        ctx.grid(fw, (32, 32, 32), f64=True)
+        t1 = time.perf_counter()
+        r = ctx.henry(fw, 298.0, 100_000, seed=k)
+        t2 = time.perf_counter()
+        fw.release()
+        if k:
+            tg.append(t1 - t0)
+            th.append(t2 - t1)
+    res["grid_ms"] = min(tg) * 1e3
+    res["henry_ms"] = min(th) * 1e3
+    res["kh_mol_m3_pa"] = r["kh_mol_m3_pa"]
+    return res
 
 
 def run_serving(ctx, args):
