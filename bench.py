@@ -436,7 +436,7 @@ def run_serving(ctx, args):
     one-job-at-a-time loop (1 slot); latency = finish - submit per job. Grid
     jobs leave their grids resident in the server's device cache."""
     from emptyroom_b200 import serve, synth
-    fws, jobs = synth.config5_stream(seconds=args.serve_seconds)
+    fws, jobs = synth.config5_stream(rate=args.serve_rate, seconds=args.serve_seconds)
     descs = [serve.framework_desc(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
 
     def schedule():
@@ -614,6 +614,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the Poisson stream (the full config-5 stream is 60 s)")
     ap.add_argument("--serve-budget-gib", type=float, default=48.0)
+    ap.add_argument("--serve-rate", type=float, default=200.0,
+                    help="mean arrivals per second of the Poisson stream (config 5: 200)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.case != "batch":
