@@ -302,6 +302,14 @@ def run_ours(args, ws, rank, local, pg):
             "unit": "Tinst/s", "frac": achieved / fp32_rate,
             "peak_source": "measured FP32 FFMA issue rate (er_probe_fp32_rate) on this GPU",
             "traffic": load_traffic(points_step)}
+    # the grid store against the measured HBM copy bandwidth (not the bound)
+    roof["grid_store_gbs"] = 4.0 * points_step / (sum(times) / len(times)) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        hbm = json.load(open(peaks_path)).get("hbm_gbs")
+        if hbm:
+            roof["hbm_peak_gbs"] = hbm
+            roof["grid_store_frac_of_measured_hbm"] = roof["grid_store_gbs"] / hbm
     line = {
         "metric": METRIC, "value": value, "unit": "pair-terms/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
