@@ -14,10 +14,10 @@
 // the lowest: the block scheduler then dispatches the CTAs of small jobs
 // ahead of those of large ones (shortest-job-first at CTA granularity, with
 // no preemption of running CTAs). The pending queue is scanned in arrival
-// order and the first job with a free slot of its class is admitted (small
-// jobs may use either class, large jobs only low-priority slots), unless the
-// oldest job has waited longer than kAgeS: then nothing overtakes it and it
-// takes any free slot. A job is admitted only when its device footprint fits
+// order (its first kScan jobs) and the first job with a free slot of its
+// class is admitted (small jobs may use either class, large jobs only
+// low-priority slots), unless the oldest job has waited longer than kAgeS:
+// then nothing overtakes it and it takes any free slot. A job is admitted only when its device footprint fits
 // the HBM budget after evicting unpinned cached grids (least recently used
 // first). One slot is the plain one-job-at-a-time loop. The budget is
 // reserved in the context's memory pool when the server is created.
@@ -64,6 +64,7 @@ struct SrvJob {
     er_job_status st{};
     int slot = -1;
     GridKey gkey{};
+    double log_cost = 0.0;  // log of the admission cost estimate (set at submission)
 };
 
 struct Slot {
@@ -77,6 +78,7 @@ struct Slot {
 };
 
 constexpr double kAgeS = 0.05;       // a job waiting longer is overtaken by none
+constexpr int kScan = 64;            // pending jobs examined per admission attempt
 
 }  // namespace
 
@@ -167,13 +169,17 @@ struct er_server {
     // Admits (or resolves) one pending job; returns whether it did.
     bool admit_one() {
         if (pending.empty()) return false;
+        bool any_free = false;
+        for (const Slot& sl : slots) any_free |= !sl.busy;
+        if (!any_free) return false;
         const double t_now = now();
         const bool aged = t_now - jobs[pending.front()].st.submit_s > kAgeS;
-        for (auto it = pending.begin(); it != pending.end(); ++it) {
+        int examined = 0;
+        for (auto it = pending.begin(); it != pending.end() && examined < kScan;
+             ++it, ++examined) {
             const uint64_t ticket = *it;
             SrvJob& j = jobs[ticket];
-            const double cost = job_cost(j.job);
-            const double lc = log(cost);
+            const double lc = j.log_cost;
             if (!cost_seen) {
                 cost_log_ema = lc;
                 cost_seen = true;
@@ -415,6 +421,7 @@ int er_server_submit(er_server* s, const er_job* job, uint64_t* ticket) {
     SrvJob j;
     j.job = *job;
     j.st.submit_s = s->now();
+    j.log_cost = log(s->job_cost(*job));
     s->jobs.emplace(t, j);
     s->pending.push_back(t);
     *ticket = t;
