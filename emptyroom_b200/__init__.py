@@ -31,6 +31,7 @@ ER_BATCH_PERSISTENT = 0
 ER_BATCH_PLAIN = 1
 ER_BATCH_HOST_OUT = 0x100
 ER_BATCH_AUTOTUNE = 0x200
+ER_BATCH_NEAR64 = 0x400
 ER_ENERGY_CAP = 1.0e30
 ER_INTERP_GRID_F64 = 0x1
 R_GAS = 8.314  # J/(mol K), src/henry.cu:169

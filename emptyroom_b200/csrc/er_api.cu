@@ -225,6 +225,8 @@ static int configure_kernels(er_ctx* ctx) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_FP32>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    ER_CUDA(ctx, cudaFuncSetAttribute(grid_persistent_kernel<PREC_NEAR64>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     return st;
 }
 
@@ -282,13 +284,19 @@ int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const int* d_st
     const size_t smem = sizeof(EngineSmem);
     int per_sm = 0;
     ER_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                     &per_sm, grid_persistent_kernel<PREC_COMP>, kThreads, smem));
+                     &per_sm,
+                     prec == PREC_NEAR64 ? grid_persistent_kernel<PREC_NEAR64>
+                                         : grid_persistent_kernel<PREC_COMP>,
+                     kThreads, smem));
     per_sm = std::max(per_sm, 1);
     const int grid = std::min<int64_t>((int64_t)ctx->num_sms * per_sm, std::max(n_items, 1));
     ER_CUDA(ctx, cudaMemsetAsync(d_head, 0, sizeof(int), ctx->stream));
     cudaStream_t st = ctx->stream;
     if (prec == PREC_FP32)
         grid_persistent_kernel<PREC_FP32><<<grid, kThreads, smem, st>>>(
+            d_tasks, d_start, n_tasks, n_items, d_head, task_left, done_dev);
+    else if (prec == PREC_NEAR64)
+        grid_persistent_kernel<PREC_NEAR64><<<grid, kThreads, smem, st>>>(
             d_tasks, d_start, n_tasks, n_items, d_head, task_left, done_dev);
     else
         grid_persistent_kernel<PREC_COMP><<<grid, kThreads, smem, st>>>(
@@ -739,6 +747,7 @@ int er_grid_sheet(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int x_index,
 struct er_batch_plan {
     er_ctx* ctx = nullptr;
     int mode = ER_BATCH_PERSISTENT;
+    int prec = 0;                  // er::PREC_COMP or er::PREC_NEAR64
     int n_jobs = 0;
     std::vector<GridTask> tasks;   // job order
     std::vector<int> order;        // queue position -> job (longest first)
@@ -767,13 +776,13 @@ static int plan_enqueue(er_batch_plan* p) {
     er_ctx* ctx = p->ctx;
     if (p->mode == ER_BATCH_PLAIN) {
         for (int i = 0; i < p->n_jobs; ++i) {
-            int st = launch_grid_plain(ctx, p->tasks[i], PREC_COMP);
+            int st = launch_grid_plain(ctx, p->tasks[i], p->prec);
             if (st != ER_OK) return st;
         }
         return ER_OK;
     }
     return launch_grid_persistent(ctx, p->d_tasks, p->d_start, p->n_jobs, p->n_items, p->d_head,
-                                  PREC_COMP);
+                                  p->prec);
 }
 
 }  // namespace er
@@ -790,13 +799,15 @@ int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool
                 er_batch_plan** out) {
     if (!ctx || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return ER_ERR_INVALID;
     const bool autotune = (mode & ER_BATCH_AUTOTUNE) != 0;
-    mode &= ~ER_BATCH_AUTOTUNE;
+    const int prec = (mode & ER_BATCH_NEAR64) ? PREC_NEAR64 : PREC_COMP;
+    mode &= ~(ER_BATCH_AUTOTUNE | ER_BATCH_NEAR64);
     if (mode != ER_BATCH_PERSISTENT && mode != ER_BATCH_PLAIN) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     *out = nullptr;
     er_batch_plan* p = new er_batch_plan();
     p->ctx = ctx;
     p->mode = mode;
+    p->prec = prec;
     p->n_jobs = n_jobs;
     std::vector<double> cost;
     for (int i = 0; i < n_jobs; ++i) {
@@ -954,7 +965,8 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
                                    (off[i + 1] - off[i]) * sizeof(float), cudaMemcpyDeviceToHost,
                                    ctx->copy_stream);
         };
-        if ((inner & ~ER_BATCH_AUTOTUNE) != ER_BATCH_PERSISTENT || n_jobs == 0) {
+        if ((inner & ~(ER_BATCH_AUTOTUNE | ER_BATCH_NEAR64)) != ER_BATCH_PERSISTENT ||
+            n_jobs == 0) {
             int st = er_grid_batch(ctx, dj.data(), n_jobs, inner);
             if (st != ER_OK) return st;
             for (int i = 0; i < n_jobs; ++i) ER_CUDA(ctx, copy_out(i));
@@ -992,7 +1004,7 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
         ER_CUDA(ctx, cudaMemcpyAsync(d_left, left.data(), (size_t)n_jobs * sizeof(int),
                                      cudaMemcpyHostToDevice, ctx->stream));
         st = launch_grid_persistent(ctx, p->d_tasks, p->d_start, n_jobs, p->n_items, p->d_head,
-                                    PREC_COMP, d_left, ctx->done_dev);
+                                    p->prec, d_left, ctx->done_dev);
         if (st != ER_OK) return st;
         cudaEvent_t fin;
         ER_CUDA(ctx, cudaEventCreateWithFlags(&fin, cudaEventDisableTiming));

@@ -136,6 +136,9 @@ typedef struct {
                                    first job of its class (atom density, grid spacing,
                                    cutoff); choices are cached in the context. A job's
                                    result then equals er_grid with that variant's flag. */
+#define ER_BATCH_NEAR64 0x400 /* or-ed into mode: the ER_PREC_NEAR64 pair sum (pairs of
+                                 atoms within 5 A of a warp's points in FP64) instead of
+                                 ER_PREC_COMP; results equal er_grid with ER_PREC_NEAR64 */
 
 /* Runs many grid jobs (uneven frameworks, probes, grid sizes). Results are
  * identical between the two modes and independent of the job mix. */

@@ -5,9 +5,10 @@ FP32 (default), NEAR64 and FP64 modes of er_grid against FP64.
 The FP64 reference over the full grid is the library's ER_PREC_FP64 grid
 (same pair set, FP64 terms and sums); it is first pinned to the FP64 oracle
 (the reference's ComputeGridSheet restated in C) on sampled points. Reported
-per mode, on E < 0 points: max and 99th-percentile absolute and relative
-error and the fraction within 1e-5 relative; on 0 <= E < 1e10: the same
-relative figures; and whether the overflow cap (E >= 1e30) marks the same
+per mode, on E < 0 points (and on E < -1 K, E < -10 K, away from the zero
+crossing where relative error is undefined): max and 99th-percentile absolute
+and relative error and the fraction within 1e-5 relative; on 0 <= E < 1e10:
+the same relative figures; and whether the overflow cap (E >= 1e30) marks the same
 points as FP64.
 
 Usage (GPU): python tests/precision_sweep.py --dims 256 [--atoms 646] --out sweep.json
@@ -35,7 +36,8 @@ def stats(e, ref):
     cap = ref >= er.ER_ENERGY_CAP
     out = {"cap_agrees": bool(np.array_equal(e >= er.ER_ENERGY_CAP, cap)),
            "n_cap": int(cap.sum())}
-    for name, m in (("neg", ref < 0), ("pos", (ref >= 0) & (ref < 1e10))):
+    for name, m in (("neg", ref < 0), ("neg_below_-1K", ref < -1.0),
+                    ("neg_below_-10K", ref < -10.0), ("pos", (ref >= 0) & (ref < 1e10))):
         d = np.abs(e[m] - ref[m])
         r = d / np.maximum(np.abs(ref[m]), 1e-30)
         out[name] = {"n": int(m.sum()),

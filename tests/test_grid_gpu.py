@@ -387,3 +387,22 @@ def test_upload_many_reports_the_bad_framework(ctx):
     items[1] = (bad,) + items[1][1:]
     with pytest.raises(er.ErError, match="framework 1"):
         ctx.upload_many(items)
+
+
+@pytest.mark.parametrize("mode", [er.ER_BATCH_PERSISTENT, er.ER_BATCH_PLAIN,
+                                  er.ER_BATCH_PERSISTENT | er.ER_BATCH_HOST_OUT])
+def test_batch_near64_equals_single_near64(ctx, mode):
+    """The precision form of the batch: every job equals er_grid with
+    ER_PREC_NEAR64, bit for bit."""
+    import torch
+    fws, ups = _batch_frameworks(ctx, n=8, seed=150)
+    host = bool(mode & er.ER_BATCH_HOST_OUT)
+    if host:
+        outs = [torch.empty(f.dims, dtype=torch.float32, pin_memory=True) for f in fws]
+    else:
+        outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
+    ctx.grid_batch([(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)],
+                   mode | er.ER_BATCH_NEAR64)
+    for u, f, o in zip(ups, fws, outs):
+        single = ctx.grid(u, f.dims, precision=er.ER_PREC_NEAR64)
+        assert np.array_equal(o.cpu().numpy(), single)
