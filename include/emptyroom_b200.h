@@ -256,15 +256,21 @@ int er_synth_positions(uint64_t seed, const double t_matrix[9], int n_atoms, dou
 
 /* ------------------------------------------------------------------ serving */
 /* A request server over one context: jobs are submitted from any host thread
- * as they arrive; a scheduler thread admits them in arrival order while a job
- * slot is free and their device footprint fits the HBM budget, and launches
- * each admitted job on its slot's stream, so jobs that arrive while others
- * run execute concurrently on the device (continuous batching). Framework
- * images and finished grids stay resident on the device (caches keyed by the
+ * as they arrive; a scheduler thread admits them while a job slot is free and
+ * their device footprint fits the HBM budget, and launches each admitted job
+ * on its slot's stream, so jobs that arrive while others run execute
+ * concurrently on the device (continuous batching). Admission is size-aware:
+ * jobs cheaper than the running median (points x atom density) go to slots
+ * created at the highest stream priority, others to low-priority slots; the
+ * oldest job is overtaken by none once it has waited 50 ms. Framework images
+ * and finished grids stay resident on the device (caches keyed by the
  * caller's framework key and the grid size); least recently used grids are
  * evicted when the budget needs room. A job's result does not depend on which
  * other jobs run beside it. With slots = 1 the server runs one job at a time
- * (the plain one-job-per-launch loop). The reference has no serving layer. */
+ * (the plain one-job-per-launch loop). The reference has no serving layer.
+ * er_server_create reserves the budget in the context's memory pool. While a
+ * server exists its scheduler thread uses the context: make no other calls on
+ * that context, and destroy the server before the context. */
 typedef struct er_server er_server;
 #define ER_JOB_GRID 1
 #define ER_JOB_HENRY 2
