@@ -347,6 +347,7 @@ def run_ours(args, ws, rank, local, pg):
     # the scaled workload)
     if ws == 1:
         line["config1"] = run_config1(ctx)
+        line["extras"] = run_extras(ctx)
     if ws == 1 and not args.no_widom:
         line["widom"] = run_widom(ctx, args)
     if ws == 1 and not args.no_serving:
@@ -363,6 +364,7 @@ def run_ours(args, ws, rank, local, pg):
 
         line["cpu_baseline"] = cpu_baseline(fws, sheet_pairs)
         line["cpu_baseline"]["config1_grid_s"] = cpu_config1_grid()
+        line["cpu_baseline"]["pockets_129cube_s"] = cpu_pockets_ref()
     ctx.close()
     return line
 
@@ -448,6 +450,81 @@ def run_config1(ctx):
     res["henry_ms"] = min(th) * 1e3
     res["kh_mol_m3_pa"] = r["kh_mol_m3_pa"]
     return res
+
+
+def run_extras(ctx):
+    """The remaining rows of the path, one config-4 cell (0.2 A, 129^3):
+    GPU pocket blocking (device grid -> device mask), the GCMC grid lookup
+    (1e7 guest positions, device in and out), and the parallel .txt grid
+    writer (host, byte-identical to the reference's format)."""
+    import tempfile
+
+    import torch
+
+    from emptyroom_b200 import files, synth
+    f = synth.config4(1, seed=4000)[0]
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    dims = f.dims
+    g = torch.empty(dims, dtype=torch.float32, device="cuda")
+    ctx.grid_device(fw, dims, g.data_ptr())
+    m = torch.empty(dims, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.ExternalStream(ctx.stream_ptr)
+
+    def tm(fn, n=5):
+        fn()
+        ctx.synchronize()
+        ts = []
+        for _ in range(n):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        return min(ts)
+
+    n_p = [0]
+
+    def pockets():
+        n_p[0] = ctx.block_pockets_device(g.data_ptr(), dims, 298.0, m.data_ptr())
+
+    t_pk = tm(pockets)
+    n_q = 10_000_000
+    pts = torch.rand((n_q, 3), dtype=torch.float64, device="cuda", generator=torch.Generator(
+        device="cuda").manual_seed(0))
+    out = torch.empty(n_q, dtype=torch.float64, device="cuda")
+    t_lk = tm(lambda: ctx.grid_interp_device(g.data_ptr(), dims, pts.data_ptr(), n_q,
+                                             out.data_ptr()))
+    host = g.cpu().numpy()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "grid.txt")
+        t0 = time.perf_counter()
+        files.write_grid_txt(path, host)
+        t_io = time.perf_counter() - t0
+        size = os.path.getsize(path)
+    fw.release()
+    return {"workload": f"config-4 cell, 0.2 A grid {list(dims)}",
+            "pockets": {"ms": t_pk * 1e3, "n_pockets": n_p[0],
+                        "points_per_s": float(np.prod(dims)) / t_pk},
+            "gcmc_lookup": {"lookups_per_s": n_q / t_lk, "ms_per_1e7": t_lk * 1e3},
+            "grid_txt_write": {"s": t_io, "bytes": size, "mb_per_s": size / t_io / 1e6}}
+
+
+def cpu_pockets_ref():
+    """The reference's FindAndBlockPockets (oracle/_ref) on the same config-4
+    grid, computed there by the oracle in FP64 (seconds for the blocking)."""
+    import oracle
+    from emptyroom_b200 import synth
+    f = synth.config4(1, seed=4000)[0]
+    E = oracle.grid(f.particles(), f.t_matrix, f.rep, f.rc2, f.dims,
+                    n_threads=os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    if oracle.ref_available():
+        oracle.ref_block_pockets(E, 298.0)
+    else:
+        oracle.block_pockets(E, 298.0)
+    return time.perf_counter() - t0
 
 
 def run_serving(ctx, args):
