@@ -230,14 +230,20 @@ static int configure_kernels(er_ctx* ctx) {
     return st;
 }
 
+int check_grid_dims(er_ctx* ctx, int nx, int ny, int nz, const char* who) {
+    if (nx < 2 || ny < 2 || nz < 2)
+        return set_error(ctx, ER_ERR_INVALID,
+                         std::string(who) + ": nx, ny, nz must be >= 2 (axes i/(N-1))");
+    if ((double)nx * ny * nz > 4.0e9)
+        return set_error(ctx, ER_ERR_LIMIT, std::string(who) + ": more than 4e9 points");
+    return ER_OK;
+}
+
 int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, float* out,
                    GridTask& t, int tile_p) {
     if (tile_p != 4 && tile_p != 8)
         return set_error(ctx, ER_ERR_INVALID, "grid: kernel variant must have P = 4 or 8");
-    if (nx < 2 || ny < 2 || nz < 2)
-        return set_error(ctx, ER_ERR_INVALID, "grid: nx, ny, nz must be >= 2 (axes i/(N-1))");
-    if ((double)nx * ny * nz > 4.0e9)
-        return set_error(ctx, ER_ERR_LIMIT, "grid: more than 4e9 points");
+    if (int st = check_grid_dims(ctx, nx, ny, nz, "grid")) return st;
     t.fw = fw.dev;
     t.cc = make_cutoff_consts(fw.rc2, 0.0, 1e-12 * 1e-12);  // min_r, src/computegridsheet.h:19
     t.nx = nx; t.ny = ny; t.nz = nz;
@@ -645,6 +651,7 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes) {
 
 int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out) {
     if (!ctx || !out) return ER_ERR_INVALID;
+    if (int st = check_grid_dims(ctx, nx, ny, nz, "grid")) return st;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const FwRecord* f = find_fw(ctx, fw_id);
     if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "grid: unknown framework id");
@@ -718,6 +725,7 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
 int er_grid_sheet(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int x_index,
                   double* out_sheet) {
     if (!ctx || !out_sheet) return ER_ERR_INVALID;
+    if (int st = check_grid_dims(ctx, nx, ny, nz, "sheet")) return st;
     if (x_index < 0 || x_index >= nx) return set_error(ctx, ER_ERR_INVALID, "sheet: x_index");
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     auto& c = ctx->sheet_cache;

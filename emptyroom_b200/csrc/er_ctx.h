@@ -110,6 +110,9 @@ int cuda_error(er_ctx* ctx, cudaError_t e, const char* what);
 const FwRecord* find_fw(er_ctx* ctx, int fw_id);
 // Cutoff constants for a framework and a CTA box diagonal (A).
 CutoffConsts make_cutoff_consts(double rc2, double box_diag, double r2min);
+// Grid dimensions accepted by every grid entry point: each >= 2 (axes
+// i / (N - 1)) and at most 4e9 points; checked before any allocation.
+int check_grid_dims(er_ctx* ctx, int nx, int ny, int nz, const char* who);
 // Fills a grid task (validates dims) and launches the plain grid kernel on `st`.
 int fill_grid_task(er_ctx* ctx, const FwRecord& fw, int nx, int ny, int nz, float* out,
                    GridTask& t, int tile_p = 4);

@@ -547,8 +547,7 @@ __global__ void __launch_bounds__(256) acc_grid_kernel(const double4* __restrict
 
 extern "C" int er_accessibility(er_ctx* ctx, int fw_id, int nx, int ny, int nz, uint8_t* out) {
     if (!ctx || !out) return ER_ERR_INVALID;
-    if (nx < 2 || ny < 2 || nz < 2)
-        return er::set_error(ctx, ER_ERR_INVALID, "accessibility: nx, ny, nz must be >= 2");
+    if (int st = er::check_grid_dims(ctx, nx, ny, nz, "accessibility")) return st;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const er::FwRecord* f = er::find_fw(ctx, fw_id);
     if (!f) return er::set_error(ctx, ER_ERR_NOT_FOUND, "accessibility: unknown framework id");
