@@ -313,17 +313,20 @@ int launch_grid_persistent(er_ctx* ctx, const GridTask* d_tasks, const int* d_st
 
 // ------------------------------------------------------------------ autotuner
 // Picks the kernel variant (4 or 8 points per thread) for a class of jobs by
-// timing both on the same sample of the job -- its first 16 x-layers, which
-// are whole bricks for both variants -- and caches the faster one per class:
-// (atoms per A^3 in half-octaves, smallest grid spacing in quarter-octaves,
-// cutoff in quarter-Angstroms).
-int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out, int* tile_p) {
+// timing both, in the precision mode the jobs run in, on the same sample of
+// the job -- its first 16 x-layers, which are whole bricks for both variants
+// -- and caches the faster one per class: (atoms per A^3 in half-octaves,
+// smallest grid spacing in quarter-octaves, cutoff in quarter-Angstroms,
+// precision mode).
+int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out, int prec,
+              int* tile_p) {
     const double rho = (double)std::max(f.n_atoms, 1) / std::max(f.volume, 1e-9);
     double h = 1e30;
     const int dims[3] = {nx, ny, nz};
     for (int d = 0; d < 3; ++d) h = std::min(h, f.cell_len[d] / std::max(dims[d] - 1, 1));
-    const std::tuple<int, int, int> key((int)lround(2.0 * log2(rho)), (int)lround(4.0 * log2(h)),
-                                        (int)lround(4.0 * sqrt(f.rc2)));
+    const std::tuple<int, int, int, int> key((int)lround(2.0 * log2(rho)),
+                                             (int)lround(4.0 * log2(h)),
+                                             (int)lround(4.0 * sqrt(f.rc2)), prec);
     auto it = ctx->tune.find(key);
     if (it != ctx->tune.end()) {
         *tile_p = it->second;
@@ -338,7 +341,7 @@ int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out
     // enough for four waves of the bigger (P = 8) bricks on this GPU, so
     // neither variant is timed on an underfilled launch.
     const int nbyz = ((ny + 2 * kWJ - 1) / (2 * kWJ)) * ((nz + 2 * kWK - 1) / (2 * kWK));
-    const int slots = 3 * ctx->num_sms;
+    const int slots = (prec == PREC_NEAR64 ? 2 : 3) * ctx->num_sms;
     const int layers = 16 * std::max(1, (4 * slots + nbyz - 1) / nbyz);
     for (int P : {4, 8}) {
         GridTask t;
@@ -348,7 +351,7 @@ int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out
         float ms_min = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             ER_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
-            st = launch_grid_plain(ctx, t, PREC_COMP);
+            st = launch_grid_plain(ctx, t, prec);
             if (st != ER_OK) return st;
             ER_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
             ER_CUDA(ctx, cudaEventSynchronize(e1));
@@ -828,7 +831,7 @@ int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool
         int tile_p = 4;
         int st = ER_OK;
         if (autotune && jobs[i].nx >= 2 && jobs[i].ny >= 2 && jobs[i].nz >= 2)
-            st = tune_tile(ctx, *f, jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].out_device,
+            st = tune_tile(ctx, *f, jobs[i].nx, jobs[i].ny, jobs[i].nz, jobs[i].out_device, prec,
                            &tile_p);
         GridTask t;
         if (st == ER_OK)

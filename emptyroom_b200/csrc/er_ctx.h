@@ -76,7 +76,7 @@ struct er_ctx {
     std::map<int, er::FwRecord> fws;
     int next_fw = 1;
     double cell_edge = 2.0;  // cell-list edge (A)
-    std::map<std::tuple<int, int, int>, int> tune;  // autotuned kernel variant per job class
+    std::map<std::tuple<int, int, int, int>, int> tune;  // autotuned kernel variant per job class
     // scratch
     er::DevBuf grid_f32;     // staging for host-bound grids
     er::DevBuf counter;      // scratch of the FP32 rate probe
