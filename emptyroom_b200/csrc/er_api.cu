@@ -774,9 +774,13 @@ struct er_batch_plan {
 
 namespace er {
 
-// Longest-first order of the jobs: bricks of denser frameworks (more atoms
-// per A^3, so more pairs per point) go first, so the tail of the persistent
-// queue holds the cheap bricks.
+// Queue order of the jobs, largest key first. For device output the key is
+// the cost per brick (atoms per A^3: denser frameworks have more pairs per
+// point), so the tail of the persistent queue holds the cheap bricks. For host
+// output it is the grid size: a grid's copy to the host starts when its last
+// brick is done, so the big grids go first and the copies left after the
+// kernel ends are the small ones. (A brick is at most about half a
+// millisecond of one CTA's work, so either order leaves a short kernel tail.)
 static void queue_order(const std::vector<double>& cost, std::vector<int>& order) {
     order.resize(cost.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
@@ -807,7 +811,7 @@ namespace er {
 // Builds a plan; with capture, the launch sequence is also captured as a graph
 // (er_batch_plan_run replays it).
 int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool capture,
-                er_batch_plan** out) {
+                er_batch_plan** out, bool host_order = false) {
     if (!ctx || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return ER_ERR_INVALID;
     const bool autotune = (mode & ER_BATCH_AUTOTUNE) != 0;
     const int prec = (mode & ER_BATCH_NEAR64) ? PREC_NEAR64 : PREC_COMP;
@@ -843,7 +847,8 @@ int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool
         }
         p->tasks.push_back(t);
         // per-brick cost ~ atom density * cutoff volume
-        cost.push_back((double)f->dev.n_img / std::max(1.0, f->volume));
+        cost.push_back(host_order ? (double)jobs[i].nx * jobs[i].ny * jobs[i].nz
+                                  : (double)f->dev.n_img / std::max(1.0, f->volume));
     }
     queue_order(cost, p->order);
     auto fail = [&](int st, const char* m) {
@@ -985,7 +990,7 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
             return ER_OK;
         }
         er_batch_plan* p = nullptr;
-        int st = plan_create(ctx, dj.data(), n_jobs, inner, false, &p);
+        int st = plan_create(ctx, dj.data(), n_jobs, inner, false, &p, true);
         if (st != ER_OK) return st;
         std::unique_ptr<er_batch_plan, void (*)(er_batch_plan*)> guard(p, er_batch_plan_destroy);
         // bricks left per queue position, and the host-visible flags
