@@ -292,7 +292,12 @@ def run_ours(args, ws, rank, local, pg):
                        er.ER_BATCH_AUTOTUNE)
         dt = time.perf_counter() - t0
         if step == 0:
-            h2d = sum(u.device_bytes for u in ups2)
+            # what er_framework_upload_many copies up: per atom its FP64
+            # position and sig2 (32 B), FP64 (C12, C6) (16 B) and FP32
+            # (C12, -C6) (8 B); per framework a 240-byte build record (copied
+            # before each of the two build passes) and a block offset (the
+            # image cell lists are built on the device)
+            h2d = sum(56 * len(it[0]) + 484 for it in host_items) + 4
             d2h = int(points_step) * 4
             hv = host.numpy()
             for k in range(2):

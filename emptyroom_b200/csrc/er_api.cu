@@ -479,21 +479,15 @@ int er_ctx_stream(er_ctx* ctx, void** stream) {
 
 namespace er {
 
-// Byte layout of one framework's device block (every array 256-byte aligned).
-struct FwLayout {
-    size_t o_par, o_id, o_cs, o_af, o_lj, total;
-};
-
-static FwLayout fw_layout(const HostFramework& hf) {
+FwLayout fw_layout(size_t n_img, size_t n_cs, size_t n_atoms) {
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-    const size_t n_img = hf.img_xyz.size();
     FwLayout L;
     const size_t s_xyz = al(std::max<size_t>(n_img, 1) * sizeof(HostImage));
     const size_t s_par = al(std::max<size_t>(n_img, 1) * 2 * sizeof(float));
     const size_t s_id = al(std::max<size_t>(n_img, 1) * sizeof(uint32_t));
-    const size_t s_cs = al(hf.cell_start.size() * sizeof(int));
-    const size_t s_af = al(std::max<size_t>(hf.atom_frac.size(), 1) * sizeof(HostImage));
-    const size_t s_lj = al(std::max<size_t>(hf.atom_lj64.size(), 2) * sizeof(double));
+    const size_t s_cs = al(n_cs * sizeof(int));
+    const size_t s_af = al(std::max<size_t>(n_atoms, 1) * sizeof(HostImage));
+    const size_t s_lj = al(std::max<size_t>(2 * n_atoms, 2) * sizeof(double));
     L.o_par = s_xyz;
     L.o_id = L.o_par + s_par;
     L.o_cs = L.o_id + s_id;
@@ -514,8 +508,9 @@ static void fw_stage(const HostFramework& hf, const FwLayout& L, char* h) {
     memcpy(h + L.o_lj, hf.atom_lj64.data(), hf.atom_lj64.size() * sizeof(double));
 }
 
-// Fills the handle record of a framework whose block is (being) copied to `block`.
-static void fw_record(const HostFramework& hf, const FwLayout& L, void* block, FwRecord& rec) {
+// Fills the handle record of a framework whose block is (being) written at `block`.
+void fw_record(const HostFramework& hf, size_t n_img, const FwLayout& L, void* block,
+               FwRecord& rec) {
     rec.block = block;
     char* b = (char*)block;
     FwDev& d = rec.dev;
@@ -525,7 +520,7 @@ static void fw_record(const HostFramework& hf, const FwLayout& L, void* block, F
     d.cell_start = (const int*)(b + L.o_cs);
     d.atom_frac = (const double4*)(b + L.o_af);
     d.atom_lj64 = (const double2*)(b + L.o_lj);
-    d.n_img = (int)hf.img_xyz.size();
+    d.n_img = (int)n_img;
     d.n_atoms = hf.n_atoms;
     for (int k = 0; k < 3; ++k) {
         d.nc[k] = hf.nc[k];
@@ -550,31 +545,28 @@ static void fw_record(const HostFramework& hf, const FwLayout& L, void* block, F
     rec.n_atoms = hf.n_atoms;
 }
 
-// Runs f(i) for i in [0, n) on up to hardware_concurrency host threads.
-template <class F>
-static void parallel_for(int n, F&& f) {
-    const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
-    std::atomic<int> next(0);
-    auto worker = [&]() {
-        for (int i; (i = next.fetch_add(1)) < n;) f(i);
-    };
-    std::vector<std::thread> th;
-    for (int t = 1; t < nt; ++t) th.emplace_back(worker);
-    worker();
-    for (auto& x : th) x.join();
-}
-
 }  // namespace er
 
 extern "C" {
 
 int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) {
     if (!ctx || !desc || !fw_id) return ER_ERR_INVALID;
-    return er_framework_upload_many(ctx, desc, 1, fw_id);
+    return host_upload_many(ctx, desc, 1, fw_id);
 }
 
 int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids) {
     if (!ctx || n < 0 || (n > 0 && (!descs || !fw_ids))) return ER_ERR_INVALID;
+    if (n == 0) return ER_OK;
+    return device_upload_many(ctx, descs, n, fw_ids);
+}
+
+}  // extern "C"
+
+namespace er {
+
+// Uploads with the image cell lists built on the host threads (one framework
+// per thread), staged into pinned memory and copied.
+int host_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids) {
     if (n == 0) return ER_OK;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     // 1. image cell lists, built on the host threads
@@ -591,7 +583,7 @@ int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n,
     std::vector<FwLayout> lay(n);
     std::vector<size_t> at(n + 1, 0);
     for (int i = 0; i < n; ++i) {
-        lay[i] = fw_layout(hfs[i]);
+        lay[i] = fw_layout(hfs[i].img_xyz.size(), hfs[i].cell_start.size(), hfs[i].atom_frac.size());
         at[i + 1] = at[i] + lay[i].total;
     }
     std::vector<void*> blocks(n, nullptr);
@@ -624,13 +616,17 @@ int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n,
     }
     for (int i = 0; i < n; ++i) {
         FwRecord rec;
-        fw_record(hfs[i], lay[i], blocks[i], rec);
+        fw_record(hfs[i], hfs[i].img_xyz.size(), lay[i], blocks[i], rec);
         const int id = ctx->next_fw++;
         ctx->fws[id] = rec;
         fw_ids[i] = id;
     }
     return ER_OK;
 }
+
+}  // namespace er
+
+extern "C" {
 
 int er_framework_release(er_ctx* ctx, int fw_id) {
     if (!ctx) return ER_ERR_INVALID;

@@ -2,7 +2,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <map>
+#include <thread>
 #include <tuple>
 #include <mutex>
 #include <string>
@@ -102,6 +105,35 @@ struct er_ctx {
 
 namespace er {
 
+struct HostFramework;
+
+// Byte layout of one framework's device block (every array 256-byte aligned):
+// images (double4), (C12, -C6) (float2), image ids (u32), cell_start
+// (ncell + 1 ints), atom_frac (double4), atom_lj64 (double2).
+struct FwLayout {
+    size_t o_par, o_id, o_cs, o_af, o_lj, total;
+};
+FwLayout fw_layout(size_t n_img, size_t n_cs, size_t n_atoms);
+// Fills the handle record of a framework whose block is (being) written at `block`.
+void fw_record(const HostFramework& hf, size_t n_img, const FwLayout& L, void* block,
+               FwRecord& rec);
+// Uploads with the image cell lists built on the host threads.
+int host_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids);
+
+// Runs f(i) for i in [0, n) on up to hardware_concurrency host threads.
+template <class F>
+void parallel_for(int n, F&& f) {
+    const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+        for (int i; (i = next.fetch_add(1)) < n;) f(i);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+}
+
 int set_error(er_ctx* ctx, int status, const std::string& msg);
 // Device memory from the context's pool, ordered on ctx->stream; the pool
 // keeps freed memory for reuse (trimmed and retried once when exhausted).
@@ -125,6 +157,12 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
                   const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
                   HenryScratch& hs, HenryOut* host_out);
 void henry_finish(const HenryOut& h, int64_t n, double temperature, er_henry_result* out);
+// Exclusive scan of n ints on `st`: out[0..n] (out[n] = the total), with
+// scan_tiles(n) ints of scratch in tile_sums.
+int scan_tiles(int n);
+int scan_exclusive(er_ctx* ctx, const int* in, int n, int* out, int* tile_sums, cudaStream_t st);
+// Builds the image cell lists of n frameworks on the device (er_build.cu).
+int device_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids);
 
 }  // namespace er
 

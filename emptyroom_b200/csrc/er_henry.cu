@@ -184,6 +184,22 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const int* __r
     }
 }
 
+int scan_tiles(int n) { return (n + kScanTile - 1) / kScanTile; }
+
+int scan_exclusive(er_ctx* ctx, const int* in, int n, int* out, int* tile_sums,
+                   cudaStream_t st) {
+    if (n <= 0) {
+        ER_CUDA(ctx, cudaMemsetAsync(out, 0, sizeof(int), st));
+        return ER_OK;
+    }
+    const int tiles = scan_tiles(n);
+    scan_tiles_kernel<<<tiles, kScanThreads, 0, st>>>(in, n, tile_sums);
+    scan_top_kernel<<<1, 1024, 0, st>>>(tile_sums, tiles, out + n);
+    scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(in, n, tile_sums, out);
+    ER_CUDA(ctx, cudaGetLastError());
+    return ER_OK;
+}
+
 __global__ void henry_scatter_kernel(const int* __restrict__ key, int n,
                                      const int* __restrict__ starts, int* __restrict__ fill,
                                      int* __restrict__ tmp) {

@@ -51,7 +51,9 @@ void perpendicular_widths(const double t[9], double w[3]) {
     w[2] = vol / sqrt(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
 }
 
-int build_framework(const er_framework_desc& d, double h, HostFramework& f, std::string& err) {
+int prepare_framework(const er_framework_desc& d, double h, HostFramework& f, std::string& err,
+                      HostImage* atom_frac, double* atom_lj64, float* atom_par, double w[3],
+                      double* keep) {
     if (d.n_atoms < 0 || (d.n_atoms > 0 && d.atoms == nullptr)) {
         err = "framework: n_atoms < 0 or atoms == NULL";
         return ER_ERR_INVALID;
@@ -72,7 +74,6 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
         err = "framework: r_cutoff_squared must be positive and finite";
         return ER_ERR_INVALID;
     }
-    double w[3];
     perpendicular_widths(d.t_matrix, w);
     if (!(w[0] > 0) || !(w[1] > 0) || !(w[2] > 0)) {
         err = "framework: degenerate cell matrix";
@@ -91,7 +92,6 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
     f.rc2 = d.r_cutoff_squared;
     f.imgs_per_atom = (int)ipa;
     f.h = h;
-    f.atom_frac.resize(d.n_atoms);
     for (int a = 0; a < d.n_atoms; ++a) {
         const er_particle& p = d.atoms[a];
         if (!std::isfinite(p.x_f) || !std::isfinite(p.y_f) || !std::isfinite(p.z_f) ||
@@ -100,31 +100,22 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
             err = "framework: atom with non-finite or negative parameters";
             return ER_ERR_INVALID;
         }
-        f.atom_frac[a] = HostImage{p.x_f, p.y_f, p.z_f, p.sig_with_adsorbate_squared};
+        atom_frac[a] = HostImage{p.x_f, p.y_f, p.z_f, p.sig_with_adsorbate_squared};
+        const double s2 = p.sig_with_adsorbate_squared;
+        const double c6l = 4.0 * p.eps_with_adsorbate * s2 * s2 * s2;
+        atom_lj64[2 * a] = c6l * s2 * s2 * s2;
+        atom_lj64[2 * a + 1] = c6l;
     }
-    f.atom_lj64.resize(2 * (size_t)d.n_atoms);
-    for (int a = 0; a < d.n_atoms; ++a) {
-        const double s2 = d.atoms[a].sig_with_adsorbate_squared;
-        const double c6 = 4.0 * d.atoms[a].eps_with_adsorbate * s2 * s2 * s2;
-        f.atom_lj64[2 * a] = c6 * s2 * s2 * s2;
-        f.atom_lj64[2 * a + 1] = c6;
-    }
-    // Keep image a + n only if it can be within rc of the grid region
-    // [0,1]^3: its fractional overshoot of slab d times the slab width w_d is a
-    // lower bound on its distance to every grid point.
-    const double rc = sqrt(d.r_cutoff_squared);
-    const double keep = rc * (1.0 + 1e-9) + 1e-6;
-    std::vector<HostImage> xyz;
-    std::vector<float> par;
-    std::vector<uint32_t> ids;
-    const double* t = f.r;  // image positions in the positioning frame
     for (int a = 0; a < d.n_atoms; ++a) {
         const er_particle& p = d.atoms[a];
+        const double s2 = p.sig_with_adsorbate_squared;
         // An atom with eps == 0 or sig == 0 adds exactly 0.0 to every sum of
-        // src/computegridsheet.h:82 (r^2 >= min_r^2 keeps s^6 finite): drop it.
-        if (p.eps_with_adsorbate == 0.0 || p.sig_with_adsorbate_squared == 0.0) continue;
-        const double s6 = p.sig_with_adsorbate_squared * p.sig_with_adsorbate_squared *
-                          p.sig_with_adsorbate_squared;
+        // src/computegridsheet.h:82 (r^2 >= min_r^2 keeps s^6 finite): it
+        // gets no images.
+        atom_par[2 * a] = 0.0f;
+        atom_par[2 * a + 1] = 0.0f;
+        if (p.eps_with_adsorbate == 0.0 || s2 == 0.0) continue;
+        const double s6 = s2 * s2 * s2;
         const double c6 = 4.0 * p.eps_with_adsorbate * s6;
         const double c12 = c6 * s6;
         float c12f = (float)c12;
@@ -134,6 +125,36 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
             return ER_ERR_LIMIT;
         }
         if (c12f == 0.0f) c12f = 1.17549435e-38f;  // keep u3 * (C12 u3 - C6) NaN-free
+        atom_par[2 * a] = c12f;
+        atom_par[2 * a + 1] = -c6f;
+    }
+    // Keep image a + n only if it can be within rc of the grid region
+    // [0,1]^3: its fractional overshoot of slab d times the slab width w_d is a
+    // lower bound on its distance to every grid point.
+    const double rc = sqrt(d.r_cutoff_squared);
+    *keep = rc * (1.0 + 1e-9) + 1e-6;
+    return ER_OK;
+}
+
+int build_framework(const er_framework_desc& d, double h, HostFramework& f, std::string& err) {
+    const int na = d.n_atoms > 0 ? d.n_atoms : 0;
+    std::vector<HostImage> af(na);
+    std::vector<double> lj(2 * (size_t)na);
+    std::vector<float> apar(2 * (size_t)na);
+    double w[3], keep = 0.0;
+    const int st = prepare_framework(d, h, f, err, af.data(), lj.data(), apar.data(), w, &keep);
+    if (st != ER_OK) return st;
+    f.atom_frac = std::move(af);
+    f.atom_lj64 = std::move(lj);
+    const int64_t ipa = f.imgs_per_atom;
+    std::vector<HostImage> xyz;
+    std::vector<float> par;
+    std::vector<uint32_t> ids;
+    const double* t = f.r;  // image positions in the positioning frame
+    for (int a = 0; a < d.n_atoms; ++a) {
+        const er_particle& p = d.atoms[a];
+        if (apar[2 * a] == 0.0f) continue;  // no images (eps == 0 or sig == 0)
+        const float c12f = apar[2 * a], nc6f = apar[2 * a + 1];
         int code = 0;
         for (int i = -d.rep[0]; i <= d.rep[0]; ++i)
             for (int j = -d.rep[1]; j <= d.rep[1]; ++j)
@@ -150,7 +171,7 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
                     im.pad = 0.0;
                     xyz.push_back(im);
                     par.push_back(c12f);
-                    par.push_back(-c6f);
+                    par.push_back(nc6f);
                     ids.push_back((uint32_t)((int64_t)a * ipa + code));
                 }
     }
@@ -171,16 +192,8 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
             lo[2] = std::min(lo[2], im.z); hi[2] = std::max(hi[2], im.z);
         }
     }
-    int64_t ncell = 1;
-    for (int k = 0; k < 3; ++k) {
-        f.cell_lo[k] = lo[k];
-        f.nc[k] = (int)floor((hi[k] - lo[k]) / h) + 1;
-        ncell *= f.nc[k];
-    }
-    if (ncell > (int64_t)64 * 1024 * 1024) {
-        err = "framework: cell list too large (cell edge too small for this cell)";
-        return ER_ERR_LIMIT;
-    }
+    int64_t ncell = 0;
+    if (int st2 = cell_grid(lo, hi, h, f, &ncell, err)) return st2;
     std::vector<int> cell(n);
     std::vector<int> count((size_t)ncell + 1, 0);
     const double inv_h = 1.0 / h;
@@ -207,6 +220,22 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
         f.img_par[2 * dst + 1] = par[2 * q + 1];
         f.img_id[dst] = ids[q];
     }
+    return ER_OK;
+}
+
+int cell_grid(const double lo[3], const double hi[3], double h, HostFramework& f, int64_t* ncell,
+              std::string& err) {
+    int64_t nc = 1;
+    for (int k = 0; k < 3; ++k) {
+        f.cell_lo[k] = lo[k];
+        f.nc[k] = (int)floor((hi[k] - lo[k]) / h) + 1;
+        nc *= f.nc[k];
+    }
+    if (nc > (int64_t)64 * 1024 * 1024) {
+        err = "framework: cell list too large (cell edge too small for this cell)";
+        return ER_ERR_LIMIT;
+    }
+    *ncell = nc;
     return ER_OK;
 }
 

@@ -32,6 +32,22 @@ struct HostFramework {
     std::vector<double> atom_lj64;      // 2 per atom: C12, C6 in FP64
 };
 
+// Validates desc and fills everything of `out` but the image cell list
+// (img_*, cell_start, nc, cell_lo stay empty): the scalars, and per atom the
+// FP64 fractional position and sig2 (atom_frac), the FP64 (C12, C6)
+// (atom_lj64) and the FP32 image coefficients (C12, -C6) in atom_par, which
+// is (0, 0) for an atom with eps == 0 or sig2 == 0 (it has no images). The
+// three per-atom arrays are written to the caller's buffers of n_atoms
+// entries. w gets the perpendicular widths, *keep the image-keep distance.
+int prepare_framework(const er_framework_desc& desc, double h, HostFramework& out,
+                      std::string& err, HostImage* atom_frac, double* atom_lj64,
+                      float* atom_par, double w[3], double* keep);
+
+// Cell grid of edge h over the bounding box [lo, hi] of the kept images:
+// sets f.cell_lo and f.nc; ER_ERR_LIMIT past 64 Mi cells.
+int cell_grid(const double lo[3], const double hi[3], double h, HostFramework& f, int64_t* ncell,
+              std::string& err);
+
 // Validates desc and builds the image cell list with cell edge h (A).
 int build_framework(const er_framework_desc& desc, double h, HostFramework& out,
                     std::string& err);

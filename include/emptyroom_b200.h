@@ -70,13 +70,15 @@ int er_ctx_stream(er_ctx* ctx, void** stream);
 
 /* ------------------------------------------------------------------ frameworks */
 /* Uploads a framework/probe pair and builds its device-resident image cell
- * list. Replaces the cudaMalloc/cudaMemcpy of FrameworkParticle[] at
- * src/writegrid.cu:187-189 and src/henry.cu:133-135. *fw_id receives a handle. */
+ * list (on the host, then copied). Replaces the cudaMalloc/cudaMemcpy of
+ * FrameworkParticle[] at src/writegrid.cu:187-189 and src/henry.cu:133-135.
+ * *fw_id receives a handle. */
 int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id);
-/* Uploads n frameworks at once: the image cell lists are built on all host
- * threads, staged in one pinned buffer and copied with one wait. On error no
- * handle is created. (No counterpart in the reference, which reads one
- * framework per process.) */
+/* Uploads n frameworks at once: only the atoms are copied (56 bytes each),
+ * and the image cell lists are built on the device, equal bit for bit to
+ * er_framework_upload's. Validation runs on the host first, with the same
+ * errors; on error no handle is created. (No counterpart in the reference,
+ * which reads one framework per process.) */
 int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids);
 int er_framework_release(er_ctx* ctx, int fw_id);
 /* Device bytes held by a framework handle. */

@@ -379,6 +379,40 @@ def test_upload_many_equals_single_uploads(ctx):
         u.release()
 
 
+def test_upload_many_device_build_edge_cases(ctx):
+    """er_framework_upload_many builds the image cell lists on the device;
+    er_framework_upload builds them on the host. The two blocks must be the
+    same on the cases the builder branches on: no atoms, atoms with eps == 0
+    (no images), a small cell with large replication, a rotated (not upper
+    triangular) cell matrix, and a call with a single framework."""
+    small = synth.make_framework(171, (8.2, 9.0, 8.6), (70, 110, 95), 30, probe="Xe")
+    base = synth.make_framework(172, (16.0, 19.0, 17.5), (75, 105, 98), 140, probe="Kr")
+    P = base.particles()
+    no_eps = P.copy()
+    no_eps[::3, 3] = 0.0  # every third atom: eps == 0
+    items = [
+        (P[:0], base.t_matrix, base.rep, base.rc2),
+        (no_eps, base.t_matrix, base.rep, base.rc2),
+        (small.particles(), small.t_matrix, small.rep, small.rc2),
+        (P, _rotated(base.t_matrix, 5), base.rep, base.rc2),
+    ]
+    assert max(small.rep) >= 2
+    dims = (13, 11, 15)
+    for batch in (items, items[3:]):
+        many = ctx.upload_many(batch)
+        for it, u in zip(batch, many):
+            single = ctx.upload(*it)
+            assert u.device_bytes == single.device_bytes
+            assert np.array_equal(ctx.grid(u, dims), ctx.grid(single, dims))
+            assert np.array_equal(ctx.count_pairs(u, dims), ctx.count_pairs(single, dims))
+            assert np.array_equal(ctx.grid(u, dims, precision=er.ER_PREC_NEAR64),
+                                  ctx.grid(single, dims, precision=er.ER_PREC_NEAR64))
+            single.release()
+        for u in many:
+            u.release()
+    assert not ctx.grid(ctx.upload_many(items[:1])[0], dims).any()
+
+
 def test_upload_many_reports_the_bad_framework(ctx):
     fws = synth.config2(n_frameworks=3, seed=131, spacing_range=(0.9, 1.6))
     items = [(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws]
