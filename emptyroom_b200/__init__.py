@@ -311,6 +311,21 @@ class Context:
             mnx, mny, mnz, ctypes.byref(res), None))
         return {k: getattr(res, k) for k, _ in ErHenryResult._fields_}
 
+    def henry_batch(self, fws, temperature, n_ins, seeds, block_dims=None):
+        """er_henry_batch: per framework (optionally) the blocking grid of
+        block_dims, its pocket mask, then er_henry with that seed; returns
+        (list of result dicts, list of pocket counts)."""
+        n = len(fws)
+        ids = (ctypes.c_int * max(n, 1))(*[f.id for f in fws])
+        sd = (ctypes.c_uint64 * max(n, 1))(*[int(s) for s in seeds])
+        res = (ErHenryResult * max(n, 1))()
+        npk = (ctypes.c_int * max(n, 1))()
+        bx, by, bz = (int(x) for x in block_dims) if block_dims is not None else (0, 0, 0)
+        self._check(_capi.lib().er_henry_batch(self._h, ids, n, float(temperature), int(n_ins),
+                                               sd, bx, by, bz, res, npk))
+        out = [{k: getattr(res[i], k) for k, _ in ErHenryResult._fields_} for i in range(n)]
+        return out, [npk[i] for i in range(n)]
+
     def block_pockets(self, grid, temperature, want_segments=False):
         """FindAndBlockPockets on a host float64 grid; returns (grid copy, n_pockets[, seg])."""
         g = np.array(grid, dtype=np.float64, copy=True, order="C")

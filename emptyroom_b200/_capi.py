@@ -86,6 +86,8 @@ SIGNATURES = {
     "er_batch_plan_tile": (c_int, [c_void_p, c_int, _ip]),
     "er_henry": (c_int, [c_void_p, c_int, c_double, c_int64, c_uint64, _u8p, c_int, c_int,
                          c_int, ctypes.POINTER(ErHenryResult), _fp]),
+    "er_henry_batch": (c_int, [c_void_p, _ip, c_int, c_double, c_int64, ctypes.POINTER(c_uint64),
+                               c_int, c_int, c_int, ctypes.POINTER(ErHenryResult), _ip]),
     "er_henry_stats_noalloc": (c_int, [c_void_p, c_void_p, c_int64, c_double,
                                        ctypes.POINTER(ErHenryResult)]),
     "er_block_pockets": (c_int, [c_void_p, _dp, c_int, c_int, c_int, c_double, _ip, _ip]),

@@ -80,7 +80,10 @@ void HostBuf::release() {
 }
 
 int set_error(er_ctx* ctx, int status, const std::string& msg) {
-    if (ctx) ctx->last_error = msg;
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->err_mu);
+        ctx->last_error = msg;
+    }
     return status;
 }
 
@@ -444,10 +447,21 @@ void er_ctx_destroy(er_ctx* ctx) {
     cudaStreamSynchronize(ctx->copy_stream);
     for (auto& kv : ctx->fws) cudaFreeAsync(kv.second.block, ctx->stream);
     ctx->fws.clear();
-    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->counter,
-                      &ctx->p_grid,   &ctx->p_lab,  &ctx->p_seg,  &ctx->p_flags,
-                      &ctx->p_misc,   &ctx->p_mask, &ctx->sheet_cache.grid, &ctx->interp};
+    DevBuf* bufs[] = {&ctx->grid_f32, &ctx->counter, &ctx->sheet_cache.grid, &ctx->interp};
     for (DevBuf* b : bufs) b->release();
+    ctx->pocket.release();
+    for (HenryPipe* p : ctx->pipes) {
+        cudaStreamSynchronize(p->stream);
+        p->hs.release();
+        p->ps.release();
+        p->grid.release();
+        p->mask.release();
+        cudaStreamSynchronize(p->stream);
+        if (p->out) cudaFreeHost(p->out);
+        cudaStreamDestroy(p->stream);
+        delete p;
+    }
+    ctx->pipes.clear();
     ctx->henry.release();
     ctx->pinned.release();
     ctx->plan_pinned.release();

@@ -68,6 +68,27 @@ struct HenryOut {
     int n_blocked;
 };
 
+// Device scratch of one pocket-blocking run (er_pockets.cu): labels,
+// segments, per-segment flags, scan/link tables, a grid copy, the FP64 grid
+// of er_block_pockets.
+struct PocketScratch {
+    DevBuf grid, lab, seg, flags, misc, mask;
+    void release() {
+        DevBuf* b[] = {&grid, &lab, &seg, &flags, &misc, &mask};
+        for (DevBuf* x : b) x->release();
+    }
+};
+
+// One pipeline of er_henry_batch: its stream and everything a framework's
+// grid -> pocket mask -> Widom run needs, so that pipelines overlap.
+struct HenryPipe {
+    cudaStream_t stream = nullptr;
+    HenryScratch hs;
+    PocketScratch ps;
+    DevBuf grid, mask;
+    HenryOut* out = nullptr;  // pinned
+};
+
 }  // namespace er
 
 struct er_ctx {
@@ -93,7 +114,10 @@ struct er_ctx {
     // Widom scratch
     er::HenryScratch henry;
     // pocket-blocking scratch
-    er::DevBuf p_grid, p_lab, p_seg, p_flags, p_misc, p_mask;
+    er::PocketScratch pocket;
+    // pipelines of er_henry_batch (created on first use)
+    std::vector<er::HenryPipe*> pipes;
+    std::mutex err_mu;  // last_error is written by er_henry_batch's workers too
     // staging of host points / results for er_grid_interp
     er::DevBuf interp;
     // device-resident grid cache for er_grid_sheet: key (fw, nx, ny, nz)
@@ -157,6 +181,12 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
                   const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
                   HenryScratch& hs, HenryOut* host_out);
 void henry_finish(const HenryOut& h, int64_t n, double temperature, er_henry_result* out);
+// Pocket mask of an FP32 device grid (er_block_pockets_device) with scratch
+// `ps` on stream `st`; synchronises `st` (the segment classification runs on
+// the host).
+int block_pockets_device_on(er_ctx* ctx, PocketScratch& ps, cudaStream_t st, const float* grid,
+                            int nx, int ny, int nz, double temperature, uint8_t* mask_out,
+                            int* n_pockets);
 // Exclusive scan of n ints on `st`: out[0..n] (out[n] = the total), with
 // scan_tiles(n) ints of scratch in tile_sums.
 int scan_tiles(int n);

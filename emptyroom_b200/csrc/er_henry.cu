@@ -457,3 +457,117 @@ extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_in
     henry_finish(h, n_ins, temperature, out);
     return ER_OK;
 }
+
+// ------------------------------------------------------------------ Widom batch
+// er_henry_batch: frameworks handed out to kHenryPipes pipelines, each a host
+// thread driving its own stream and scratch (HenryPipe), so that one
+// framework's grid, pocket labelling, binning and host round trips run while
+// another's energy kernel holds the SMs. Every step is the single-call code
+// (fill_grid_task + the plain grid kernel as er_grid, block_pockets_device_on
+// as er_block_pockets_device, henry_enqueue as er_henry), so each result
+// equals the single calls' bit for bit.
+namespace er {
+namespace {
+
+constexpr int kHenryPipes = 3;
+
+int henry_one(er_ctx* ctx, HenryPipe& P, const FwRecord& fw, double temperature, int64_t n_ins,
+              uint64_t seed, const int bd[3], er_henry_result* out, int* n_pockets) {
+    const cudaStream_t st = P.stream;
+    const uint8_t* mask = nullptr;
+    int npk = 0;
+    if (bd[0]) {
+        const size_t pts = (size_t)bd[0] * bd[1] * bd[2];
+        if (P.grid.ensure_on(pts * sizeof(float), ctx->pool, st) ||
+            P.mask.ensure_on(pts, ctx->pool, st))
+            return set_error(ctx, ER_ERR_NOMEM, "henry batch: grid/mask allocation failed");
+        GridTask t;
+        int s = fill_grid_task(ctx, fw, bd[0], bd[1], bd[2], (float*)P.grid.ptr, t, 4);
+        if (s == ER_OK) s = launch_grid_plain_on(ctx, t, PREC_COMP, st);
+        if (s == ER_OK)
+            s = block_pockets_device_on(ctx, P.ps, st, (const float*)P.grid.ptr, bd[0], bd[1],
+                                        bd[2], temperature, (uint8_t*)P.mask.ptr, &npk);
+        if (s != ER_OK) return s;
+        mask = (const uint8_t*)P.mask.ptr;
+    }
+    int s = henry_enqueue(ctx, fw, temperature, (int)n_ins, seed, mask, bd[0], bd[1], bd[2], st,
+                          P.hs, P.out);
+    if (s != ER_OK) return s;
+    ER_CUDA(ctx, cudaStreamSynchronize(st));
+    henry_finish(*P.out, n_ins, temperature, out);
+    if (n_pockets) *n_pockets = npk;
+    return ER_OK;
+}
+
+}  // namespace
+}  // namespace er
+
+extern "C" int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
+                              int64_t n_insertions, const uint64_t* seeds, int block_nx,
+                              int block_ny, int block_nz, er_henry_result* results,
+                              int* n_pockets) {
+    if (!ctx || n < 0 || (n > 0 && (!fw_ids || !seeds || !results))) return ER_ERR_INVALID;
+    if (n == 0) return ER_OK;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    int st = henry_check(ctx, temperature, n_insertions, nullptr, 0, 0, 0);
+    if (st != ER_OK) return st;
+    const bool blocking = block_nx != 0 || block_ny != 0 || block_nz != 0;
+    const int bd[3] = {blocking ? block_nx : 0, blocking ? block_ny : 0, blocking ? block_nz : 0};
+    if (blocking) {
+        if ((st = check_grid_dims(ctx, block_nx, block_ny, block_nz, "henry batch")) != ER_OK)
+            return st;
+        if ((int64_t)block_nx * block_ny * block_nz >= (int64_t)INT32_MAX)
+            return set_error(ctx, ER_ERR_LIMIT, "henry batch: blocking grid must have < 2^31 points");
+    }
+    std::vector<const FwRecord*> fr(n);
+    for (int k = 0; k < n; ++k)
+        if (!(fr[k] = find_fw(ctx, fw_ids[k])))
+            return set_error(ctx, ER_ERR_NOT_FOUND,
+                             "henry batch: unknown framework id (entry " + std::to_string(k) + ")");
+    const int np = std::min(n, kHenryPipes);
+    while ((int)ctx->pipes.size() < np) {
+        HenryPipe* p = new HenryPipe();
+        if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaMallocHost((void**)&p->out, sizeof(HenryOut)) != cudaSuccess) {
+            cudaGetLastError();
+            if (p->stream) cudaStreamDestroy(p->stream);
+            delete p;
+            return set_error(ctx, ER_ERR_CUDA, "henry batch: stream creation failed");
+        }
+        ctx->pipes.push_back(p);
+    }
+    // the pipelines' scratch and the framework blocks come from the pool in
+    // stream order: order every pipeline after the work already queued
+    cudaEvent_t ready;
+    ER_CUDA(ctx, cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    ER_CUDA(ctx, cudaEventRecord(ready, ctx->stream));
+    for (int p = 0; p < np; ++p) ER_CUDA(ctx, cudaStreamWaitEvent(ctx->pipes[p]->stream, ready, 0));
+    cudaEventDestroy(ready);
+    std::atomic<int> next(0), stop(0);
+    std::vector<int> status(np, ER_OK);
+    auto work = [&](int p) {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            status[p] = set_error(ctx, ER_ERR_CUDA, "henry batch: cudaSetDevice failed");
+            stop = 1;
+            return;
+        }
+        for (int k; !stop && (k = next.fetch_add(1)) < n;) {
+            const int s = henry_one(ctx, *ctx->pipes[p], *fr[k], temperature, n_insertions,
+                                    seeds[k], bd, &results[k], n_pockets ? &n_pockets[k] : nullptr);
+            if (s != ER_OK) {
+                status[p] = s;
+                stop = 1;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    for (int p = 1; p < np; ++p) th.emplace_back(work, p);
+    work(0);
+    for (auto& t : th) t.join();
+    for (int p = 0; p < np; ++p) {
+        cudaStreamSynchronize(ctx->pipes[p]->stream);
+        if (status[p] != ER_OK) return status[p];
+    }
+    return ER_OK;
+}

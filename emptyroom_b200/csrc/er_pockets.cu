@@ -334,24 +334,25 @@ static int classify_segments(int n_seg, const std::vector<unsigned long long>& l
     return n_pockets;
 }
 
-// Steps 2-6 on a labelled grid; fills ctx->p_seg (segment per point) and
-// ctx->p_flags (pocket flag per segment, device) and returns the pocket count.
-static int segment_and_classify(er_ctx* ctx, int nx, int ny, int nz, int* n_pockets) {
+// Steps 2-6 on a labelled grid (ps.lab), on stream st; fills ps.seg (segment
+// per point) and ps.flags (pocket flag per segment, device) and returns the
+// pocket count.
+static int segment_and_classify(er_ctx* ctx, PocketScratch& ps, cudaStream_t st, int nx, int ny,
+                                int nz, int* n_pockets) {
     const int64_t n = (int64_t)nx * ny * nz;
-    cudaStream_t st = ctx->stream;
-    int* lab = (int*)ctx->p_lab.ptr;
-    int* seg = (int*)ctx->p_seg.ptr;
+    int* lab = (int*)ps.lab.ptr;
+    int* seg = (int*)ps.seg.ptr;
     const int gb = std::max(1, std::min<int>((int)((n + 255) / 256), ctx->num_sms * 16));
     cc_union<<<gb, 256, 0, st>>>(lab, nx, ny, nz);
     cc_compress<<<gb, 256, 0, st>>>(lab, n);
     const int nblk = (int)((n + kScanItems - 1) / kScanItems);
     // p_misc: block counts (nblk) | block offsets (nblk + 1) | link count | table | list
-    int* bcount = (int*)ctx->p_misc.ptr;
+    int* bcount = (int*)ps.misc.ptr;
     int* boff = bcount + nblk;
     int* nlink = boff + nblk + 1;
     cc_root_counts<<<nblk, 1024, 0, st>>>(lab, n, bcount);
     cc_scan_small<<<1, 1024, 0, st>>>(bcount, boff, nblk);
-    int* rank = (int*)ctx->p_grid.ptr;  // reuse: ranks live only until cc_segments
+    int* rank = (int*)ps.grid.ptr;  // reuse: ranks live only until cc_segments
     cc_root_ranks<<<nblk, 1024, 0, st>>>(lab, n, boff, rank);
     cc_segments<<<gb, 256, 0, st>>>(lab, rank, n, seg);
     ER_CUDA(ctx, cudaGetLastError());
@@ -363,7 +364,7 @@ static int segment_and_classify(er_ctx* ctx, int nx, int ny, int nz, int* n_pock
     while (tsize < 2 * faces) tsize <<= 1;
     const size_t misc_ints = (size_t)(2 * nblk + 2);
     const size_t tab_off = ((misc_ints * sizeof(int) + 255) / 256) * 256;
-    unsigned long long* table = (unsigned long long*)((char*)ctx->p_misc.ptr + tab_off);
+    unsigned long long* table = (unsigned long long*)((char*)ps.misc.ptr + tab_off);
     unsigned long long* list = table + tsize;
     ER_CUDA(ctx, cudaMemsetAsync(table, 0xff, tsize * sizeof(unsigned long long), st));
     ER_CUDA(ctx, cudaMemsetAsync(nlink, 0, sizeof(int), st));
@@ -375,24 +376,29 @@ static int segment_and_classify(er_ctx* ctx, int nx, int ny, int nz, int* n_pock
     ER_CUDA(ctx, cudaMemcpyAsync(&nl, nlink, sizeof(int), cudaMemcpyDeviceToHost, st));
     ER_CUDA(ctx, cudaStreamSynchronize(st));
     std::vector<unsigned long long> links(nl);
-    if (nl)
-        ER_CUDA(ctx, cudaMemcpy(links.data(), list, nl * sizeof(unsigned long long),
-                                cudaMemcpyDeviceToHost));
+    if (nl) {
+        ER_CUDA(ctx, cudaMemcpyAsync(links.data(), list, nl * sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, st));
+        ER_CUDA(ctx, cudaStreamSynchronize(st));
+    }
     // a fixed order makes the host pass independent of the insertion order
     std::sort(links.begin(), links.end());
     std::vector<unsigned char> pocket;
     const int np = classify_segments(n_seg, links, pocket);
     if (np < 0) return set_error(ctx, ER_ERR_INVALID, "pockets: malformed face link");
-    if (ctx->p_flags.ensure(std::max<size_t>(pocket.size(), 1)) != ER_OK)
+    if (ps.flags.ensure_on(std::max<size_t>(pocket.size(), 1), ctx->pool, st) != ER_OK)
         return set_error(ctx, ER_ERR_NOMEM, "pockets: flag allocation");
-    if (!pocket.empty())
-        ER_CUDA(ctx, cudaMemcpy(ctx->p_flags.ptr, pocket.data(), pocket.size(),
-                                cudaMemcpyHostToDevice));
+    if (!pocket.empty()) {
+        ER_CUDA(ctx, cudaMemcpyAsync(ps.flags.ptr, pocket.data(), pocket.size(),
+                                     cudaMemcpyHostToDevice, st));
+        ER_CUDA(ctx, cudaStreamSynchronize(st));  // `pocket` is freed on return
+    }
     *n_pockets = np;
     return ER_OK;
 }
 
-static int ensure_pocket_scratch(er_ctx* ctx, int nx, int ny, int nz, size_t grid_bytes) {
+static int ensure_pocket_scratch(er_ctx* ctx, PocketScratch& ps, cudaStream_t st, int nx, int ny,
+                                 int nz, size_t grid_bytes) {
     const int64_t n = (int64_t)nx * ny * nz;
     const int64_t faces = (int64_t)ny * nz + (int64_t)nx * nz + (int64_t)nx * ny;
     int64_t tsize = 1024;
@@ -401,9 +407,10 @@ static int ensure_pocket_scratch(er_ctx* ctx, int nx, int ny, int nz, size_t gri
     const size_t misc_ints = (size_t)(2 * nblk + 2);
     const size_t tab_off = ((misc_ints * sizeof(int) + 255) / 256) * 256;
     const size_t misc = tab_off + (size_t)(tsize + faces) * sizeof(unsigned long long);
-    if (ctx->p_lab.ensure(n * sizeof(int)) || ctx->p_seg.ensure(n * sizeof(int)) ||
-        ctx->p_grid.ensure(std::max<size_t>(grid_bytes, n * sizeof(int))) ||
-        ctx->p_misc.ensure(misc))
+    cudaMemPool_t pool = ctx->pool;
+    if (ps.lab.ensure_on(n * sizeof(int), pool, st) || ps.seg.ensure_on(n * sizeof(int), pool, st) ||
+        ps.grid.ensure_on(std::max<size_t>(grid_bytes, n * sizeof(int)), pool, st) ||
+        ps.misc.ensure_on(misc, pool, st))
         return set_error(ctx, ER_ERR_NOMEM, "pockets: device scratch allocation failed");
     return ER_OK;
 }
@@ -427,50 +434,62 @@ extern "C" int er_block_pockets(er_ctx* ctx, double* grid, int nx, int ny, int n
     if (stt != ER_OK) return stt;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const int64_t n = (int64_t)nx * ny * nz;
-    if ((stt = ensure_pocket_scratch(ctx, nx, ny, nz, n * sizeof(double))) != ER_OK) return stt;
-    if (ctx->p_mask.ensure(n * sizeof(double)) != ER_OK)
-        return set_error(ctx, ER_ERR_NOMEM, "pockets: grid allocation failed");
-    double* dE = (double*)ctx->p_mask.ptr;
+    PocketScratch& ps = ctx->pocket;
     cudaStream_t st = ctx->stream;
+    if ((stt = ensure_pocket_scratch(ctx, ps, st, nx, ny, nz, n * sizeof(double))) != ER_OK)
+        return stt;
+    if (ps.mask.ensure_on(n * sizeof(double), ctx->pool, st) != ER_OK)
+        return set_error(ctx, ER_ERR_NOMEM, "pockets: grid allocation failed");
+    double* dE = (double*)ps.mask.ptr;
     ER_CUDA(ctx, cudaMemcpyAsync(dE, grid, n * sizeof(double), cudaMemcpyHostToDevice, st));
     const int gb = std::max(1, std::min<int>((int)((n + 255) / 256), ctx->num_sms * 16));
-    cc_init_f64<<<gb, 256, 0, st>>>(dE, n, 15.0 * temperature, (int*)ctx->p_lab.ptr);
+    cc_init_f64<<<gb, 256, 0, st>>>(dE, n, 15.0 * temperature, (int*)ps.lab.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     int np = 0;
-    if ((stt = segment_and_classify(ctx, nx, ny, nz, &np)) != ER_OK) return stt;
-    cc_block_f64<<<gb, 256, 0, st>>>(dE, (const int*)ctx->p_seg.ptr, n,
-                                     (const unsigned char*)ctx->p_flags.ptr);
+    if ((stt = segment_and_classify(ctx, ps, st, nx, ny, nz, &np)) != ER_OK) return stt;
+    cc_block_f64<<<gb, 256, 0, st>>>(dE, (const int*)ps.seg.ptr, n,
+                                     (const unsigned char*)ps.flags.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     ER_CUDA(ctx, cudaMemcpyAsync(grid, dE, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (segments_out)
-        ER_CUDA(ctx, cudaMemcpyAsync(segments_out, ctx->p_seg.ptr, n * sizeof(int),
+        ER_CUDA(ctx, cudaMemcpyAsync(segments_out, ps.seg.ptr, n * sizeof(int),
                                      cudaMemcpyDeviceToHost, st));
     ER_CUDA(ctx, cudaStreamSynchronize(st));
     *n_pockets = np;
     return ER_OK;
 }
 
-extern "C" int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, int ny, int nz,
-                                       double temperature, uint8_t* pocket_mask_out,
-                                       int* n_pockets) {
-    if (!ctx || !grid || !pocket_mask_out || !n_pockets) return ER_ERR_INVALID;
+namespace er {
+
+int block_pockets_device_on(er_ctx* ctx, PocketScratch& ps, cudaStream_t st, const float* grid,
+                            int nx, int ny, int nz, double temperature, uint8_t* mask_out,
+                            int* n_pockets) {
     int stt = check_dims(ctx, nx, ny, nz, temperature);
     if (stt != ER_OK) return stt;
-    ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const int64_t n = (int64_t)nx * ny * nz;
-    if ((stt = ensure_pocket_scratch(ctx, nx, ny, nz, 0)) != ER_OK) return stt;
-    cudaStream_t st = ctx->stream;
+    if ((stt = ensure_pocket_scratch(ctx, ps, st, nx, ny, nz, 0)) != ER_OK) return stt;
     const int gb = std::max(1, std::min<int>((int)((n + 255) / 256), ctx->num_sms * 16));
-    cc_init_f32<<<gb, 256, 0, st>>>(grid, n, 15.0 * temperature, (int*)ctx->p_lab.ptr);
+    cc_init_f32<<<gb, 256, 0, st>>>(grid, n, 15.0 * temperature, (int*)ps.lab.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     int np = 0;
-    if ((stt = segment_and_classify(ctx, nx, ny, nz, &np)) != ER_OK) return stt;
-    cc_block_mask<<<gb, 256, 0, st>>>(pocket_mask_out, (const int*)ctx->p_seg.ptr, n,
-                                      (const unsigned char*)ctx->p_flags.ptr);
+    if ((stt = segment_and_classify(ctx, ps, st, nx, ny, nz, &np)) != ER_OK) return stt;
+    cc_block_mask<<<gb, 256, 0, st>>>(mask_out, (const int*)ps.seg.ptr, n,
+                                      (const unsigned char*)ps.flags.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     ER_CUDA(ctx, cudaStreamSynchronize(st));
     *n_pockets = np;
     return ER_OK;
+}
+
+}  // namespace er
+
+extern "C" int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, int ny, int nz,
+                                       double temperature, uint8_t* pocket_mask_out,
+                                       int* n_pockets) {
+    if (!ctx || !grid || !pocket_mask_out || !n_pockets) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    return block_pockets_device_on(ctx, ctx->pocket, ctx->stream, grid, nx, ny, nz, temperature,
+                                   pocket_mask_out, n_pockets);
 }
 
 // ------------------------------------------------------------------ accessibility
@@ -553,21 +572,21 @@ extern "C" int er_accessibility(er_ctx* ctx, int fw_id, int nx, int ny, int nz, 
     if (!f) return er::set_error(ctx, ER_ERR_NOT_FOUND, "accessibility: unknown framework id");
     const int64_t n = (int64_t)nx * ny * nz;
     const int nimg = 27 * f->n_atoms;
-    if (ctx->p_lab.ensure(std::max<size_t>((size_t)nimg, 1) * sizeof(double4)) ||
-        ctx->p_seg.ensure((size_t)n))
+    if (ctx->pocket.lab.ensure(std::max<size_t>((size_t)nimg, 1) * sizeof(double4)) ||
+        ctx->pocket.seg.ensure((size_t)n))
         return er::set_error(ctx, ER_ERR_NOMEM, "accessibility: scratch allocation failed");
     er::AccParams P;
     for (int k = 0; k < 9; ++k) P.t[k] = f->t[k];
     P.nx = nx; P.ny = ny; P.nz = nz;
     cudaStream_t st = ctx->stream;
-    double4* img = (double4*)ctx->p_lab.ptr;
+    double4* img = (double4*)ctx->pocket.lab.ptr;
     if (nimg > 0)
         er::acc_images_kernel<<<std::max(1, std::min((nimg + 255) / 256, ctx->num_sms * 8)), 256,
                                 0, st>>>(f->dev.atom_frac, f->n_atoms, P, img);
     er::acc_grid_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(img, nimg, P,
-                                                                     (uint8_t*)ctx->p_seg.ptr);
+                                                                     (uint8_t*)ctx->pocket.seg.ptr);
     ER_CUDA(ctx, cudaGetLastError());
-    ER_CUDA(ctx, cudaMemcpyAsync(out, ctx->p_seg.ptr, (size_t)n, cudaMemcpyDeviceToHost, st));
+    ER_CUDA(ctx, cudaMemcpyAsync(out, ctx->pocket.seg.ptr, (size_t)n, cudaMemcpyDeviceToHost, st));
     ER_CUDA(ctx, cudaStreamSynchronize(st));
     return ER_OK;
 }

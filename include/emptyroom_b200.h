@@ -183,6 +183,22 @@ int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t
              const uint8_t* block_mask, int mnx, int mny, int mnz, er_henry_result* out,
              float* energies_out);
 
+/* Widom insertions for n frameworks: the henry tool's per-structure run
+ * (src/henry.cu:63-174, one structure per process there) for many structures
+ * in one call. For entry k: when the blocking dims are non-zero (each >= 2),
+ * the FP32 energy grid of block_nx x block_ny x block_nz points (as er_grid,
+ * ER_PREC_COMP), its pocket mask (as er_block_pockets_device, pocketblocking.cc:
+ * 126-391) and er_henry of fw_ids[k] with seed seeds[k] and that mask; with
+ * all three dims 0, er_henry alone. The frameworks run on up to three
+ * concurrent pipelines (a stream, scratch and a host thread each, kept by the
+ * context), so that one framework's grid, labelling, binning and host round
+ * trips overlap another's energy kernel. Each results[k] (and n_pockets[k],
+ * when n_pockets is not NULL) equals the single calls' bit for bit. On an
+ * error the remaining entries are not run. */
+int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
+                   int64_t n_insertions, const uint64_t* seeds, int block_nx, int block_ny,
+                   int block_nz, er_henry_result* results, int* n_pockets);
+
 /* Widom statistics of energies the caller already holds on the device,
  * computed without allocating anything: no counterpart in the reference.
  * For callers that cannot call cudaMalloc -- a code that reserves all of its

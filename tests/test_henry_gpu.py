@@ -125,3 +125,60 @@ def test_henry_device_mask_pipeline(ctx):
     assert r["n_blocked"] == o["n_blocked"]
     kh_o = _kh(o["sum_w"], n, T)
     assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
+
+
+def _sequential(ctx, fws, T, n, seeds, dims):
+    """The single-call pipeline: er_grid (device) -> er_block_pockets_device
+    -> er_henry with the device mask; or er_henry alone."""
+    import torch
+    out, pockets = [], []
+    for fw, s in zip(fws, seeds):
+        if dims is None:
+            out.append(ctx.henry(fw, T, n, s))
+            pockets.append(0)
+            continue
+        g = torch.empty(dims, dtype=torch.float32, device="cuda")
+        m = torch.empty(dims, dtype=torch.uint8, device="cuda")
+        ctx.grid_device(fw, dims, g.data_ptr())
+        pockets.append(ctx.block_pockets_device(g.data_ptr(), dims, T, m.data_ptr()))
+        out.append(ctx.henry_device_mask(fw, T, n, s, m.data_ptr(), dims))
+    return out, pockets
+
+
+@pytest.mark.parametrize("dims", [None, (33, 33, 33)])
+def test_henry_batch_equals_single_calls(ctx, dims):
+    """er_henry_batch runs frameworks on concurrent pipelines; every entry
+    must equal the single calls bit for bit (seven frameworks of different
+    sizes, more than there are pipelines), twice in a row."""
+    T = 298.0
+    fws = []
+    for k, na in enumerate([424, 120, 800, 50, 424, 300, 610]):
+        f = synth.make_framework(40 + k, (25.8, 25.8, 25.8), (90, 90, 90), na, probe="Xe")
+        fws.append(ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2))
+    seeds = [7 + 3 * k for k in range(len(fws))]
+    n = 60000
+    ref, ref_p = _sequential(ctx, fws, T, n, seeds, dims)
+    for _ in range(2):
+        got, got_p = ctx.henry_batch(fws, T, n, seeds, block_dims=dims)
+        assert got_p == ref_p
+        for a, b in zip(got, ref):
+            assert a == b
+    if dims is not None:
+        assert sum(ref_p) > 0 and any(r["n_blocked"] > 0 for r in ref)
+
+
+def test_henry_batch_errors(ctx):
+    import emptyroom_b200 as er
+    f, P, fw = _fw(ctx, 3, n_atoms=100)
+    assert ctx.henry_batch([], 298.0, 100, []) == ([], [])
+    with pytest.raises(er.ErError):
+        ctx.henry_batch([fw], -1.0, 100, [1])
+    with pytest.raises(er.ErError):
+        ctx.henry_batch([fw], 298.0, 100, [1], block_dims=(1, 8, 8))
+
+    class Gone:
+        id = 987654
+    with pytest.raises(er.ErError, match="entry 1"):
+        ctx.henry_batch([fw, Gone()], 298.0, 100, [1, 2])
+    # the context stays usable
+    assert ctx.henry_batch([fw], 298.0, 1000, [5])[0][0] == ctx.henry(fw, 298.0, 1000, 5)
