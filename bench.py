@@ -729,8 +729,8 @@ def main():
     ap.add_argument("--no-widom", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--widom-frameworks", type=int, default=64)
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
-                    help="length of the Poisson stream (the full config-5 stream is 60 s)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="length of the Poisson stream (config 5: 60 s)")
     ap.add_argument("--serve-budget-gib", type=float, default=48.0)
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="mean arrivals per second of the Poisson stream (config 5: 200)")

@@ -177,6 +177,8 @@ int launch_grid_plain_on(er_ctx* ctx, const GridTask& t, int prec, cudaStream_t 
 // given, the reduction and the blocked count are copied there asynchronously.
 int henry_check(er_ctx* ctx, double temperature, int64_t n_ins, const uint8_t* block_mask,
                 int mnx, int mny, int mnz);
+// Grows the per-insertion scratch of `hs` to hold n insertions (stream order).
+int henry_reserve(er_ctx* ctx, HenryScratch& hs, int64_t n, cudaStream_t st);
 int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, uint64_t seed,
                   const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
                   HenryScratch& hs, HenryOut* host_out);

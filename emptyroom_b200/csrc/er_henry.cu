@@ -300,6 +300,17 @@ __global__ void __launch_bounds__(256) henry_final_kernel(const Lse* __restrict_
 }
 
 
+int henry_reserve(er_ctx* ctx, HenryScratch& hs, int64_t n, cudaStream_t st) {
+    const size_t N = (size_t)n;
+    cudaMemPool_t pool = ctx->pool;
+    if (hs.pts.ensure_on(3 * N * sizeof(double), pool, st) ||
+        hs.bin.ensure_on(N * sizeof(int), pool, st) ||
+        hs.order.ensure_on(N * sizeof(int), pool, st) ||
+        hs.tmp.ensure_on(N * sizeof(int), pool, st) || hs.e.ensure_on(N * sizeof(float), pool, st))
+        return set_error(ctx, ER_ERR_NOMEM, "henry: device scratch allocation failed");
+    return ER_OK;
+}
+
 int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, uint64_t seed,
                   const uint8_t* block_mask, int mnx, int mny, int mnz, cudaStream_t st,
                   HenryScratch& hs, HenryOut* host_out) {

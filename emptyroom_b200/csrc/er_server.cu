@@ -53,7 +53,8 @@ struct SrvFw {
 
 struct SrvGrid {
     float* ptr = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;  // the grid
+    size_t cap = 0;    // its buffer (a recycled buffer may be larger)
     uint64_t last_use = 0;
     int pins = 0;
     bool ready = false;
@@ -119,10 +120,37 @@ struct er_server {
                     victim = it;
             if (victim == grids.end()) return false;
             cudaFreeAsync(victim->second.ptr, st);
-            bytes_grid -= victim->second.bytes;
+            bytes_grid -= victim->second.cap;
             grids.erase(victim);
         }
         return true;
+    }
+
+    // With the budget full, a grid of `need` bytes takes over the buffer of the
+    // least recently used idle grid whose buffer holds it with at most 25 %
+    // to spare (failing that, at most 100 %), instead of freeing grids to the
+    // pool and allocating: grid sizes vary continuously, and a pool whose
+    // memory is cut into grids of other sizes must map new memory for the
+    // request (measured stalls of up to 0.7 s on the request path). Returns
+    // nullptr when no such grid exists.
+    float* recycle(size_t need, size_t* cap) {
+        if (used() + need <= budget) return nullptr;
+        auto victim = grids.end();
+        for (size_t spare : {need / 4, need}) {
+            for (auto it = grids.begin(); it != grids.end(); ++it) {
+                const SrvGrid& g = it->second;
+                if (g.pins == 0 && g.ready && g.cap >= need && g.cap - need <= spare &&
+                    (victim == grids.end() || g.last_use < victim->second.last_use))
+                    victim = it;
+            }
+            if (victim != grids.end()) break;
+        }
+        if (victim == grids.end()) return nullptr;
+        float* p = victim->second.ptr;
+        *cap = victim->second.cap;
+        bytes_grid -= victim->second.cap;
+        grids.erase(victim);
+        return p;
     }
 
     void finish(SrvJob& j, int status) {
@@ -247,14 +275,26 @@ struct er_server {
         const er::FwRecord* fr = er::find_fw(ctx, f->second.fw_id);
         // footprint
         size_t need = 0;
+        int64_t h_cap = 0;
         if (job.kind == ER_JOB_GRID) {
             need = (size_t)job.nx * job.ny * job.nz * sizeof(float);
         } else {
-            const size_t want = (size_t)job.n_insertions * 41 + (4u << 20);
+            // a slot's Widom scratch grows with headroom (to the next power
+            // of two of insertions, at most 1.5x the job): a few growths per
+            // slot, early, instead of one per larger job (each a pool
+            // allocation that can stall once the pool's memory is cut into
+            // grids)
+            h_cap = (int64_t)1 << 20;
+            while (h_cap < job.n_insertions) h_cap <<= 1;
+            h_cap = std::max<int64_t>(job.n_insertions,
+                                      std::min<int64_t>(h_cap, job.n_insertions + job.n_insertions / 2));
+            const size_t want = (size_t)h_cap * 41 + (4u << 20);
             const size_t have = sl.hs.bytes();
             need = want > have ? want - have : 0;
         }
-        if (!make_room(need, sl.stream)) {
+        size_t rcap = 0;
+        float* rbuf = job.kind == ER_JOB_GRID ? recycle(need, &rcap) : nullptr;
+        if (!rbuf && !make_room(need, sl.stream)) {
             // nothing left to evict: wait for running jobs, or fail if none run
             bool any_busy = false;
             for (const Slot& s : slots) any_busy |= s.busy;
@@ -269,8 +309,10 @@ struct er_server {
         if (job.kind == ER_JOB_GRID) {
             SrvGrid g;
             g.bytes = need;
-            if (cudaMallocFromPoolAsync((void**)&g.ptr, g.bytes, ctx->pool, sl.stream) !=
-                cudaSuccess) {
+            g.cap = rbuf ? rcap : need;
+            g.ptr = rbuf;
+            if (!rbuf && cudaMallocFromPoolAsync((void**)&g.ptr, g.bytes, ctx->pool, sl.stream) !=
+                             cudaSuccess) {
                 cudaGetLastError();
                 st = ER_ERR_NOMEM;
             } else {
@@ -286,7 +328,7 @@ struct er_server {
                 if (st == ER_OK) {
                     g.pins = 1;
                     g.last_use = tick;
-                    bytes_grid += g.bytes;
+                    bytes_grid += g.cap;
                     grids[j.gkey] = g;
                 } else {
                     cudaFreeAsync(g.ptr, sl.stream);
@@ -294,6 +336,7 @@ struct er_server {
             }
         } else {
             st = er::henry_check(ctx, job.temperature, job.n_insertions, nullptr, 0, 0, 0);
+            if (st == ER_OK) st = er::henry_reserve(ctx, sl.hs, h_cap, sl.stream);
             if (st == ER_OK)
                 st = er::henry_enqueue(ctx, *fr, job.temperature, (int)job.n_insertions, job.seed,
                                        nullptr, 0, 0, 0, sl.stream, sl.hs, sl.pinned);
@@ -404,6 +447,20 @@ int er_server_create(er_ctx* ctx, size_t hbm_budget_bytes, int slots, er_server*
             want /= 2;
         }
         cudaStreamSynchronize(ctx->stream);
+    }
+    // Each slot's Widom scratch is reserved now as well (an eighth of the
+    // budget over all slots, at most 2^24 insertions per slot; counted in the
+    // budget): Henry jobs up to that size never grow it on the request path,
+    // where the pool's memory may already be cut up by grids.
+    {
+        const int64_t fit = (int64_t)(hbm_budget_bytes / 8 / (size_t)slots / 41);
+        int64_t cap = 0;
+        for (int64_t c = (int64_t)1 << 16; c <= std::min<int64_t>(fit, (int64_t)1 << 24); c <<= 1)
+            cap = c;
+        if (cap > 0)
+            for (Slot& sl : s->slots)
+                if (er::henry_reserve(ctx, sl.hs, cap, sl.stream) != ER_OK) break;
+        for (Slot& sl : s->slots) cudaStreamSynchronize(sl.stream);
     }
     s->thr = std::thread([s]() { s->run(); });
     *out = s;
