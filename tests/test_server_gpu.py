@@ -97,6 +97,14 @@ def test_grid_cache_and_eviction(ctx):
         with pytest.raises(serve.ServerError):
             srv.grid_ptr(ts[0])
         srv.grid_ptr(ts[-1])
+    # with the budget full, later grids take over evicted grids' buffers
+    # (slightly larger ones): every result is still the single call's
+    ups = [ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2) for f, _ in fws]
+    for k in range(6):
+        dk = (40, 40, 40 - k)
+        assert np.array_equal(keep[k].numpy(), ctx.grid(ups[k % 2], dk))
+    for u in ups:
+        u.release()
 
 
 def test_job_larger_than_budget_fails_cleanly(ctx):
