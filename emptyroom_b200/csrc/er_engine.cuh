@@ -864,10 +864,26 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
         double nacc[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) nacc[p] = 0.0;
-        for (int q = 0; q < n_near; ++q) {
-            const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
+        if (Pol::kLattice) {
+            // a lattice lane's points share y and z: dy^2 + dz^2 once per atom
+            for (int q = 0; q < n_near; ++q) {
+                const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
+                const double dy = qy[0] - a.y, dz = qz[0] - a.z;
+                const double yz = fma(dz, dz, dy * dy);
 #pragma unroll
-            for (int p = 0; p < P; ++p) nacc[p] += pair64(a, qx[p], qy[p], qz[p], cc.r2min);
+                for (int p = 0; p < P; ++p) {
+                    const double dx = qx[p] - a.x;
+                    const double u = __drcp_rn(fmax(fma(dx, dx, yz), cc.r2min));
+                    const double u3 = u * u * u;
+                    nacc[p] += u3 * fma(a.c12, u3, -a.c6);
+                }
+            }
+        } else {
+            for (int q = 0; q < n_near; ++q) {
+                const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
+#pragma unroll
+                for (int p = 0; p < P; ++p) nacc[p] += pair64(a, qx[p], qy[p], qz[p], cc.r2min);
+            }
         }
 #pragma unroll
         for (int p = 0; p < P; ++p) tot_at(s, p) += nacc[p];
