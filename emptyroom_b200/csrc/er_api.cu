@@ -129,11 +129,13 @@ CutoffConsts make_cutoff_consts(double rc2, double /*box_diag*/, double r2min) {
 }
 
 // ------------------------------------------------------------------ kernels
-// Three CTAs per SM (24 warps): the FP32 variants fit 80 registers; the FP64
-// variants (NEAR64, FP64) keep two.
+// Three CTAs per SM (24 warps) at 80 registers. NEAR64 spills some of its
+// FP64 near-pair state at that limit and is still faster than at two CTAs
+// (128 registers): 385.5 against 399.2 ms on the 256-framework batch. FP64
+// (all pairs in FP64, a reference mode) keeps two.
 template <int PREC>
 constexpr int grid_min_blocks() {
-    return (PREC == PREC_NEAR64 || PREC == PREC_FP64) ? 2 : 3;
+    return PREC == PREC_FP64 ? 2 : 3;
 }
 
 template <int PREC, int P>
@@ -344,7 +346,7 @@ int tune_tile(er_ctx* ctx, const FwRecord& f, int nx, int ny, int nz, float* out
     // enough for four waves of the bigger (P = 8) bricks on this GPU, so
     // neither variant is timed on an underfilled launch.
     const int nbyz = ((ny + 2 * kWJ - 1) / (2 * kWJ)) * ((nz + 2 * kWK - 1) / (2 * kWK));
-    const int slots = (prec == PREC_NEAR64 ? 2 : 3) * ctx->num_sms;
+    const int slots = 3 * ctx->num_sms;
     const int layers = 16 * std::max(1, (4 * slots + nbyz - 1) / nbyz);
     for (int P : {4, 8}) {
         GridTask t;
