@@ -283,10 +283,14 @@ int er_synth_positions(uint64_t seed, const double t_matrix[9], int n_atoms, dou
  * oldest job is overtaken by none once it has waited 50 ms. Framework images
  * and finished grids stay resident on the device (caches keyed by the
  * caller's framework key and the grid size); least recently used grids are
- * evicted when the budget needs room. A job's result does not depend on which
- * other jobs run beside it. With slots = 1 the server runs one job at a time
- * (the plain one-job-per-launch loop). The reference has no serving layer.
- * er_server_create reserves the budget in the context's memory pool. While a
+ * evicted when the budget needs room; with the budget full, a new grid takes
+ * over the buffer of an idle grid that holds it (at most twice its size)
+ * before any grid memory goes back to the pool. A job's result does not
+ * depend on which other jobs run beside it. With slots = 1 the server runs one
+ * job at a time (the plain one-job-per-launch loop). The reference has no
+ * serving layer. er_server_create reserves the budget in the context's memory
+ * pool and each slot's Widom scratch (an eighth of the budget over all slots,
+ * at most 2^24 insertions per slot; it counts against the budget). While a
  * server exists its scheduler thread uses the context: make no other calls on
  * that context, and destroy the server before the context. */
 typedef struct er_server er_server;
