@@ -21,17 +21,17 @@ ER_OUT_HOST = 0x0
 ER_OUT_DEVICE = 0x1
 ER_OUT_F32 = 0x0
 ER_OUT_F64 = 0x2
-ER_PREC_COMP = 0x0
+ER_PREC_NEAR64 = 0x0  # default: near pairs in FP64
+ER_PREC_COMP = 0x08
 ER_PREC_FP32 = 0x10
 ER_PREC_FP64 = 0x20
 ER_COUNT_PAIRS = 0x40
 ER_TILE_P8 = 0x80
-ER_PREC_NEAR64 = 0x08
 ER_BATCH_PERSISTENT = 0
 ER_BATCH_PLAIN = 1
 ER_BATCH_HOST_OUT = 0x100
 ER_BATCH_AUTOTUNE = 0x200
-ER_BATCH_NEAR64 = 0x400
+ER_BATCH_COMP = 0x400
 ER_ENERGY_CAP = 1.0e30
 ER_INTERP_GRID_F64 = 0x1
 R_GAS = 8.314  # J/(mol K), src/henry.cu:169
@@ -216,7 +216,7 @@ class Context:
         self._check(_capi.lib().er_framework_upload_many(self._h, arr, n, ids))
         return [Framework(self, ids[i], len(keep[i])) for i in range(n)]
 
-    def grid(self, fw, dims, precision=ER_PREC_COMP, f64=False):
+    def grid(self, fw, dims, precision=ER_PREC_NEAR64, f64=False):
         """Host grid (nx, ny, nz) as float32 (or float64)."""
         nx, ny, nz = (int(x) for x in dims)
         out = np.empty((nx, ny, nz), dtype=np.float64 if f64 else np.float32)
@@ -225,7 +225,7 @@ class Context:
                                         out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
-    def grid_device(self, fw, dims, out_ptr, precision=ER_PREC_COMP, f64=False):
+    def grid_device(self, fw, dims, out_ptr, precision=ER_PREC_NEAR64, f64=False):
         """Grid into a caller-owned device buffer (e.g. a torch tensor's data_ptr())."""
         nx, ny, nz = (int(x) for x in dims)
         flags = ER_OUT_DEVICE | (ER_OUT_F64 if f64 else ER_OUT_F32) | precision

@@ -19,6 +19,9 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 
+# largest n er_henry_stats_noalloc accepts (ER_HENRY_STATS_NOALLOC_MAX_N)
+ER_HENRY_STATS_NOALLOC_MAX_N = 2147483647
+
 
 class ErParticle(ctypes.Structure):
     _fields_ = [("x_f", c_double), ("y_f", c_double), ("z_f", c_double),

@@ -504,12 +504,14 @@ FwLayout fw_layout(size_t n_img, size_t n_cs, size_t n_atoms) {
     const size_t s_cs = al(n_cs * sizeof(int));
     const size_t s_af = al(std::max<size_t>(n_atoms, 1) * sizeof(HostImage));
     const size_t s_lj = al(std::max<size_t>(2 * n_atoms, 2) * sizeof(double));
+    const size_t s_ilj = al(std::max<size_t>(n_img, 1) * 2 * sizeof(double));
     L.o_par = s_xyz;
     L.o_id = L.o_par + s_par;
     L.o_cs = L.o_id + s_id;
     L.o_af = L.o_cs + s_cs;
     L.o_lj = L.o_af + s_af;
-    L.total = L.o_lj + s_lj;
+    L.o_ilj = L.o_lj + s_lj;
+    L.total = L.o_ilj + s_ilj;
     return L;
 }
 
@@ -522,6 +524,7 @@ static void fw_stage(const HostFramework& hf, const FwLayout& L, char* h) {
     memcpy(h + L.o_cs, hf.cell_start.data(), hf.cell_start.size() * sizeof(int));
     memcpy(h + L.o_af, hf.atom_frac.data(), hf.atom_frac.size() * sizeof(HostImage));
     memcpy(h + L.o_lj, hf.atom_lj64.data(), hf.atom_lj64.size() * sizeof(double));
+    memcpy(h + L.o_ilj, hf.img_lj64.data(), n_img * 2 * sizeof(double));
 }
 
 // Fills the handle record of a framework whose block is (being) written at `block`.
@@ -536,6 +539,7 @@ void fw_record(const HostFramework& hf, size_t n_img, const FwLayout& L, void* b
     d.cell_start = (const int*)(b + L.o_cs);
     d.atom_frac = (const double4*)(b + L.o_af);
     d.atom_lj64 = (const double2*)(b + L.o_lj);
+    d.img_lj64 = (const double2*)(b + L.o_ilj);
     d.n_img = (int)n_img;
     d.n_atoms = hf.n_atoms;
     for (int k = 0; k < 3; ++k) {
@@ -671,10 +675,10 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
     const FwRecord* f = find_fw(ctx, fw_id);
     if (!f) return set_error(ctx, ER_ERR_NOT_FOUND, "grid: unknown framework id");
     const int tile_p = (flags & ER_TILE_P8) ? 8 : 4;
-    const int prec = (flags & ER_COUNT_PAIRS)   ? PREC_COUNT
-                     : (flags & ER_PREC_FP32)   ? PREC_FP32
-                     : (flags & ER_PREC_NEAR64) ? PREC_NEAR64
-                                                : PREC_COMP;
+    const int prec = (flags & ER_COUNT_PAIRS) ? PREC_COUNT
+                     : (flags & ER_PREC_FP32) ? PREC_FP32
+                     : (flags & ER_PREC_COMP) ? PREC_COMP
+                                              : PREC_NEAR64;
     const size_t npts = (size_t)nx * ny * nz;
     const bool dev_out = (flags & ER_OUT_DEVICE) != 0;
     const bool f64 = (flags & ER_OUT_F64) != 0;
@@ -682,7 +686,7 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
         // FP64 pair terms and sums, written as FP64
         if (!f64)
             return set_error(ctx, ER_ERR_INVALID, "grid: ER_PREC_FP64 needs ER_OUT_F64");
-        if (flags & (ER_COUNT_PAIRS | ER_PREC_FP32 | ER_PREC_NEAR64))
+        if (flags & (ER_COUNT_PAIRS | ER_PREC_FP32 | ER_PREC_COMP))
             return set_error(ctx, ER_ERR_INVALID, "grid: conflicting precision flags");
         double* d64 = (double*)out;
         if (!dev_out) {
@@ -770,7 +774,7 @@ int er_grid_sheet(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int x_index,
 struct er_batch_plan {
     er_ctx* ctx = nullptr;
     int mode = ER_BATCH_PERSISTENT;
-    int prec = 0;                  // er::PREC_COMP or er::PREC_NEAR64
+    int prec = 0;                  // er::PREC_NEAR64 (default) or er::PREC_COMP
     int n_jobs = 0;
     std::vector<GridTask> tasks;   // job order
     std::vector<int> order;        // queue position -> job (longest first)
@@ -826,8 +830,8 @@ int plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode, bool
                 er_batch_plan** out, bool host_order = false) {
     if (!ctx || !out || (n_jobs > 0 && !jobs) || n_jobs < 0) return ER_ERR_INVALID;
     const bool autotune = (mode & ER_BATCH_AUTOTUNE) != 0;
-    const int prec = (mode & ER_BATCH_NEAR64) ? PREC_NEAR64 : PREC_COMP;
-    mode &= ~(ER_BATCH_AUTOTUNE | ER_BATCH_NEAR64);
+    const int prec = (mode & ER_BATCH_COMP) ? PREC_COMP : PREC_NEAR64;
+    mode &= ~(ER_BATCH_AUTOTUNE | ER_BATCH_COMP);
     if (mode != ER_BATCH_PERSISTENT && mode != ER_BATCH_PLAIN) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     *out = nullptr;
@@ -993,7 +997,7 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
                                    (off[i + 1] - off[i]) * sizeof(float), cudaMemcpyDeviceToHost,
                                    ctx->copy_stream);
         };
-        if ((inner & ~(ER_BATCH_AUTOTUNE | ER_BATCH_NEAR64)) != ER_BATCH_PERSISTENT ||
+        if ((inner & ~(ER_BATCH_AUTOTUNE | ER_BATCH_COMP)) != ER_BATCH_PERSISTENT ||
             n_jobs == 0) {
             int st = er_grid_batch(ctx, dj.data(), n_jobs, inner);
             if (st != ER_OK) return st;

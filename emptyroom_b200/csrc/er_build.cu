@@ -59,6 +59,7 @@ struct BuildFw {
     int* cell_start;
     double4* atom_frac;
     double2* atom_lj64;
+    double2* img_lj64;
 };
 
 __device__ __forceinline__ unsigned long long order_key(double x) {
@@ -90,8 +91,9 @@ __device__ __forceinline__ double overshoot(double f) {
 // Candidate q of framework F: whether it is kept, and then its position.
 __device__ __forceinline__ bool image_of(const BuildFw& F, const double4* __restrict__ af,
                                          const float2* __restrict__ ap, long long q, double& x,
-                                         double& y, double& z, float2& par) {
+                                         double& y, double& z, float2& par, int* atom = nullptr) {
     const int a = (int)(q / F.ipa);
+    if (atom) *atom = a;
     const int code = (int)(q - (long long)a * F.ipa);
     par = ap[F.atom0 + a];
     if (par.x == 0.0f) return false;  // eps == 0 or sig == 0: no images
@@ -210,19 +212,21 @@ __global__ void build_starts_kernel(const BuildFw* __restrict__ fws, int g0, int
 __global__ void __launch_bounds__(kBuildThreads)
     build_scatter_kernel(const BuildFw* __restrict__ fws, const int* __restrict__ blk0, int g0,
                          int g1, const double4* __restrict__ af, const float2* __restrict__ ap,
-                         int* __restrict__ fill) {
+                         const double2* __restrict__ lj, int* __restrict__ fill) {
     const int b = blk0[g0] + blockIdx.x;
     const int f = block_fw(blk0, g0, g1, b);
     const BuildFw& F = fws[f];
     const long long q = (long long)(b - blk0[f]) * kBuildThreads + threadIdx.x;
     double x, y, z;
     float2 par;
-    if (q < F.cand && image_of(F, af, ap, q, x, y, z, par)) {
+    int a = 0;
+    if (q < F.cand && image_of(F, af, ap, q, x, y, z, par, &a)) {
         const int c = cell_of(F, x, y, z);
         const int dst = F.cell_start[c] + atomicAdd(&fill[F.cell0 + c], 1);
         F.img_xyz[dst] = make_double4(x, y, z, 0.0);
         F.img_par[dst] = par;
         F.img_id[dst] = (uint32_t)q;
+        F.img_lj64[dst] = lj[F.atom0 + a];
     }
 }
 
@@ -238,16 +242,19 @@ __global__ void build_sort_kernel(const BuildFw* __restrict__ fws, int g0, int g
             const uint32_t id = F.img_id[u];
             const double4 p = F.img_xyz[u];
             const float2 pr = F.img_par[u];
+            const double2 l = F.img_lj64[u];
             int v = u - 1;
             while (v >= b && F.img_id[v] > id) {
                 F.img_id[v + 1] = F.img_id[v];
                 F.img_xyz[v + 1] = F.img_xyz[v];
                 F.img_par[v + 1] = F.img_par[v];
+                F.img_lj64[v + 1] = F.img_lj64[v];
                 --v;
             }
             F.img_id[v + 1] = id;
             F.img_xyz[v + 1] = p;
             F.img_par[v + 1] = pr;
+            F.img_lj64[v + 1] = l;
         }
     }
 }
@@ -419,6 +426,7 @@ int device_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* 
         F.cell_start = (int*)(b + lay[i].o_cs);
         F.atom_frac = (double4*)(b + lay[i].o_af);
         F.atom_lj64 = (double2*)(b + lay[i].o_lj);
+        F.img_lj64 = (double2*)(b + lay[i].o_ilj);
     }
     // groups of frameworks whose cells and images fit one scan
     std::vector<int> gstart(1, 0);
@@ -467,7 +475,7 @@ int device_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* 
         if (e != cudaSuccess) break;
         if (gblk > 0)
             build_scatter_kernel<<<gblk, kBuildThreads, 0, st>>>(d_fw, d_b0, g0, g1, d_af, d_ap,
-                                                                 d_counts);
+                                                                 d_lj, d_counts);
         build_sort_kernel<<<grid_for(C), 256, 0, st>>>(d_fw, g0, g1, (int)C);
         const int64_t ga = atom0[g1] - atom0[g0];
         if (ga > 0)

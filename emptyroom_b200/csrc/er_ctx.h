@@ -133,9 +133,10 @@ struct HostFramework;
 
 // Byte layout of one framework's device block (every array 256-byte aligned):
 // images (double4), (C12, -C6) (float2), image ids (u32), cell_start
-// (ncell + 1 ints), atom_frac (double4), atom_lj64 (double2).
+// (ncell + 1 ints), atom_frac (double4), atom_lj64 (double2), and the FP64
+// (C12, C6) of every image (double2, the near pairs of the NEAR64 mode).
 struct FwLayout {
-    size_t o_par, o_id, o_cs, o_af, o_lj, total;
+    size_t o_par, o_id, o_cs, o_af, o_lj, o_ilj, total;
 };
 FwLayout fw_layout(size_t n_img, size_t n_cs, size_t n_atoms);
 // Fills the handle record of a framework whose block is (being) written at `block`.

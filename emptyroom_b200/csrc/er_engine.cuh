@@ -28,8 +28,11 @@
 //  * Shell pairs whose FP32 r^2 lies within a proven error window of rc^2 are
 //    re-decided in FP64 with the reference's own expression order, so the set
 //    of summed pairs equals the FP64 reference's set exactly.
-//  * Accumulation: FP32 over chunks of 64 atoms, chunks summed in FP64
-//    (ER_PREC_COMP), or FP32 over the whole list (ER_PREC_FP32).
+//  * Accumulation: FP32 over chunks of 64 atoms, chunk sums added into FP64
+//    per-point totals (ER_PREC_COMP, ER_PREC_NEAR64), or FP32 over the whole
+//    list (ER_PREC_FP32). ER_PREC_NEAR64 (the default) evaluates the pairs of
+//    atoms within kNearR of a warp's points in FP64: those large terms carry
+//    the FP32 error where they cancel to a small |E|.
 #pragma once
 #include <float.h>
 #include <math.h>
@@ -46,7 +49,8 @@ constexpr int kWJ = 4, kWK = 8;            // lanes of a warp sub-brick along j,
 constexpr int kPMax = 8;                   // largest P any policy uses
 constexpr int kMaxCand = 1024;             // CTA candidate capacity per flush
 constexpr int kRowChunk = kThreads;        // cell rows examined per producer pass
-constexpr int kAccChunk = 64;              // atoms per FP32 partial sum
+constexpr int kAccChunk = 64;              // atoms per FP32 partial sum (shell lists,
+                                           // and every list of ER_PREC_COMP)
 constexpr float kEnergyCap = 1.0e30f;      // overflow cap (ER_ENERGY_CAP)
 
 // PREC_COUNT writes the number of in-cutoff pair terms per point instead of
@@ -61,9 +65,15 @@ struct PrecTraits {
     static constexpr bool comp = PREC == PREC_COMP || PREC == PREC_NEAR64;
     static constexpr bool near64 = PREC == PREC_NEAR64;
     static constexpr bool fp64 = PREC == PREC_FP64;
+    // Atoms per FP32 partial sum of an inner list. Once NEAR64 has taken the
+    // near terms to FP64, the rounding of the FP32 partial sums (its error
+    // grows with the chunk length times the partial's magnitude) is what is
+    // left: 16-atom partials keep every E < -10 K point of the 256-framework
+    // batch within 1e-5 of FP64, 64-atom ones leave 82 of 1.4e8 above it.
+    static constexpr int inner_chunk = PREC == PREC_NEAR64 ? 16 : 64;
 };
 
-constexpr int kNearCap = 128;     // near-list capacity per warp (overflow stays FP32)
+constexpr int kNearCap = 256;     // near-list capacity per warp (overflow stays FP32)
 constexpr int kRec = 3;           // borderline shell atoms recorded per thread and flush
                                   // (10-bit list positions packed in one register)
 constexpr float kNearR = 5.0f;    // near radius (A) from the warp box
@@ -82,7 +92,9 @@ struct __align__(32) EngineSmem {
     int cid[kMaxCand];                     // their image indices (FP64 paths)
     unsigned short wl[kWarps][kMaxCand];   // per-warp inner (front) / shell (back) lists of
                                            // byte offsets into cand
-    unsigned short wn[kWarps][kNearCap];   // per-warp near lists (PREC_NEAR64)
+    unsigned short wn[kWarps][kNearCap];   // per-warp near lists (PREC_NEAR64): atoms inside
+                                           // the cutoff for every point (front) and atoms
+                                           // crossing it (back)
     double tot[kPMax][kThreads];           // FP64 per-point sums, [p][thread]
     int row_beg[kRowChunk];
     int row_off[kRowChunk];
@@ -195,7 +207,6 @@ static __device__ __noinline__ bool exact_in_cutoff(const FwDev& fw, const doubl
     return r2 < fw.rc2;
 }
 
-// FP64 pair term of image gid at a point q given relative to the CTA centre o.
 // One atom image for FP64 pair terms: position relative to the CTA centre and
 // FP64 (C12, C6).
 struct Atom64 {
@@ -204,11 +215,12 @@ struct Atom64 {
 __device__ __forceinline__ Atom64 atom64(const FwDev& fw, int gid, double o0, double o1,
                                          double o2) {
     const double4 a = fw.img_xyz[gid];
-    const int atom = (int)(fw.img_id[gid] / (uint32_t)fw.imgs_per_atom);
-    const double2 lj = fw.atom_lj64[atom];
+    const double2 lj = fw.img_lj64[gid];
     return Atom64{a.x - o0, a.y - o1, a.z - o2, lj.x, lj.y};
 }
-// FP64 pair term of atom a at a point q (both relative to the CTA centre).
+// FP64 pair term of atom a at a point q (both relative to the CTA centre),
+// with the correctly rounded reciprocal (ER_PREC_FP64, the reference mode of
+// the precision sweeps).
 __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, double qz,
                                          double r2min) {
     const double dx = qx - a.x, dy = qy - a.y, dz = qz - a.z;
@@ -217,6 +229,26 @@ __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, 
     const double u = __drcp_rn(r2);
     const double u3 = u * u * u;
     return u3 * fma(a.c12, u3, -a.c6);
+}
+// 1/x in FP64 for the near pairs of PREC_NEAR64 by Newton's method for the
+// reciprocal: from the hardware seed y0 = rcp.approx.ftz.f64(x) (relative
+// error e0 < 2^-16), one third-order step y = y0 (1 + e + e^2), e = 1 - x y0,
+// leaves a relative error of order e0^3 plus a few FP64 roundings, i.e.
+// within a few ulps of 1/x. x is a squared distance, clamped to >= min_r^2 >
+// 0 by the caller, so the seed is finite and normal.
+__device__ __forceinline__ double rcp64_nr(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+}
+// FP64 pair term of a near pair (PREC_NEAR64): r^2 from dx and the shared
+// dy^2 + dz^2, reciprocal by rcp64_nr.
+__device__ __forceinline__ double near_term64(double dx, double yz, double c12, double c6,
+                                              double r2min) {
+    const double u = rcp64_nr(fmax(fma(dx, dx, yz), r2min));
+    const double u3 = u * u * u;
+    return u3 * fma(c12, u3, -c6);
 }
 
 // FP32 r^2 of the generic form (each point has its own x, y, z) and of the
@@ -367,6 +399,19 @@ __device__ __forceinline__ double& tot_at(EngineSmem& s, int p) {
     return s.tot[p][threadIdx.x];
 }
 
+// Folds FP32 chunk sums into FP64 registers.
+template <int M>
+__device__ __forceinline__ void fold_regs(double* acc64, f2_t* acc2) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+        float a0, a1;
+        f2_unpack(acc2[m], a0, a1);
+        acc64[2 * m] += (double)a0;
+        acc64[2 * m + 1] += (double)a1;
+        acc2[m] = 0ull;
+    }
+}
+
 // Folds FP32 chunk sums into the FP64 totals.
 template <int M>
 __device__ __forceinline__ void fold_packed(EngineSmem& s, f2_t* acc2) {
@@ -393,11 +438,14 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
                                               int n_in, Lane<Pol, PREC>& L) {
     constexpr int M = Pol::kP / 2;
     constexpr bool kComp = PrecTraits<PREC>::comp;
+    constexpr int kChunk = PrecTraits<PREC>::inner_chunk;
     f2_t px2[M], acc2[M];
+    double acc64[2 * M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
         px2[m] = f2_pack(L.px[2 * m], L.px[2 * m + 1]);
         acc2[m] = 0ull;
+        acc64[2 * m] = acc64[2 * m + 1] = 0.0;
     }
     const f2_t one2 = f2_pack(1.0f, 1.0f);
     const float py = L.py[0], pz = L.pz[0];
@@ -428,16 +476,17 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
     };
     int q = 0;
     while (q < n_in) {
-        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
-        for (; q + 1 < qe; q += 2) {  // q is even here: chunks are 64 entries
+        const int qe = kComp ? min(q + kChunk, n_in) : n_in;
+        for (; q + 1 < qe; q += 2) {  // q is even here: chunks have an even length
             const unsigned two = wl32[q >> 1];
             atom(two & 0xffffu);
             atom(two >> 16);
         }
         if (q < qe) atom(wl[q++]);
-        if (kComp) fold_packed<M>(s, acc2);
+        fold_regs<M>(acc64, acc2);
     }
-    if (!kComp) fold_packed<M>(s, acc2);
+#pragma unroll
+    for (int p = 0; p < 2 * M; ++p) tot_at(s, p) += acc64[p];
 }
 
 // Lattice shell list: cutoff tested per pair (mask 1.0 / 0.0), and the
@@ -590,7 +639,7 @@ __device__ __forceinline__ int generic_packed_lists(EngineSmem& s, const unsigne
     };
     int q = 0;
     while (q < n_in) {
-        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
+        const int qe = kComp ? min(q + PrecTraits<PREC>::inner_chunk, n_in) : n_in;
         for (; q < qe; ++q) inner_atom(wl[q]);
         if (kComp) fold_packed<M>(s, acc2);
     }
@@ -616,7 +665,7 @@ __device__ __forceinline__ int generic_lists(EngineSmem& s, const unsigned short
     for (int p = 0; p < P; ++p) acc[p] = 0.f;
     int q = 0;
     while (q < n_in) {
-        const int qe = kComp ? min(q + kAccChunk, n_in) : n_in;
+        const int qe = kComp ? min(q + PrecTraits<PREC>::inner_chunk, n_in) : n_in;
 #pragma unroll 2
         for (; q < qe; ++q) {
             const Cand& cd = *reinterpret_cast<const Cand*>(
@@ -731,10 +780,13 @@ static __device__ __noinline__ void recheck_borderline(EngineSmem& s, const Pol&
     }
 }
 
+// Kept out of line: the producer's loop state (box, cell ranges, counters)
+// is saved once around the call instead of staying live in registers
+// through the pair loops.
 template <class Pol, int PREC>
-__device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
-                                           const CutoffConsts& cc, int n_cand,
-                                           Lane<Pol, PREC>& L) {
+static __device__ __noinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
+                                               const CutoffConsts& cc, int n_cand,
+                                               Lane<Pol, PREC>& L) {
     constexpr int P = Pol::kP;
     constexpr bool kNear = PrecTraits<PREC>::near64;
     constexpr bool kF64 = PrecTraits<PREC>::fp64;
@@ -743,7 +795,7 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
     unsigned short* wl = s.wl[w];
     unsigned short* wn = s.wn[w];
     // --- split candidates into inner / shell (/ near) lists for this warp's box
-    int n_in = 0, n_sh = 0, n_near = 0;
+    int n_in = 0, n_sh = 0, n_ni = 0, n_ns = 0;
     const unsigned lt = (1u << lane) - 1u;
     const float rnear2 = kNearR * kNearR;
     const float wl0x = s.wbox[w][0], wl0y = s.wbox[w][1], wl0z = s.wbox[w][2];
@@ -764,18 +816,30 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
             const float dmax2 = fx * fx + fy * fy + fz * fz;
             in = dmax2 < cc.rin2;
             sh = !in && dmin2 < cc.rout2;
-            nr = kNear && in && dmin2 < rnear2;
+            nr = kNear && dmin2 < rnear2;
         }
         const unsigned short off = (unsigned short)(c * (int)sizeof(Cand));
         if (kNear) {
-            const unsigned bn = __ballot_sync(0xffffffffu, nr);
-            const int at = n_near + __popc(bn & lt);
-            if (nr && at >= kNearCap) nr = false;  // overflow: stays on the FP32 inner list
-            if (nr) {
-                wn[at] = off;
+            // near atoms inside the cutoff for every point of the warp go to the
+            // front of wn, near atoms crossing it (large warp boxes) to the back;
+            // past kNearCap entries they stay on the FP32 lists
+            const bool ni = nr && in, ns = nr && sh;
+            const unsigned bni = __ballot_sync(0xffffffffu, ni);
+            const unsigned bns = __ballot_sync(0xffffffffu, ns);
+            const int room = kNearCap - n_ni - n_ns;
+            const int ti = min(__popc(bni), room);
+            const int ts = min(__popc(bns), room - ti);
+            const int ai = __popc(bni & lt), as = __popc(bns & lt);
+            if (ni && ai < ti) {
+                wn[n_ni + ai] = off;
                 in = false;
             }
-            n_near = min(kNearCap, n_near + __popc(bn));
+            if (ns && as < ts) {
+                wn[kNearCap - 1 - (n_ns + as)] = off;
+                sh = false;
+            }
+            n_ni += ti;
+            n_ns += ts;
         }
         const unsigned bi = __ballot_sync(0xffffffffu, in);
         const unsigned bs = __ballot_sync(0xffffffffu, sh);
@@ -853,40 +917,79 @@ __device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const 
     // --- exact re-decision of borderline shell pairs (rare); lanes without a
     // flagged point idle through it
     if (nrec > 0) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, nrec, rec, L);
-    // --- near list in FP64: exact positions (FP64 images and points relative
-    // to the CTA centre) and FP64 (C12, C6); all near atoms are inner atoms.
-    // Atom-outer order: one atom's loads serve the lane's P points.
-    if (kNear && n_near > 0) {
-        double qx[P], qy[P], qz[P], o0, o1, o2;
+    // --- near lists in FP64: exact positions (FP64 images and points relative
+    // to the CTA centre) and FP64 (C12, C6). Atom-outer order: one atom's loads
+    // serve up to kNearP of the lane's points, so a pass keeps 2 kNearP FP64
+    // registers of point state.
+    if (kNear && n_ni + n_ns > 0) {
+        constexpr int kNearP = P < 4 ? P : 4;
+        double o0, o1, o2;
         cta_centre(s, o0, o1, o2);
+#pragma unroll 1
+        for (int p0 = 0; p0 < P; p0 += kNearP) {
+            double qx[kNearP], qy[Pol::kLattice ? 1 : kNearP], qz[Pol::kLattice ? 1 : kNearP];
+            double nacc[kNearP];
 #pragma unroll
-        for (int p = 0; p < P; ++p) point64(p, qx[p], qy[p], qz[p]);
-        double nacc[P];
-#pragma unroll
-        for (int p = 0; p < P; ++p) nacc[p] = 0.0;
-        if (Pol::kLattice) {
-            // a lattice lane's points share y and z: dy^2 + dz^2 once per atom
-            for (int q = 0; q < n_near; ++q) {
+            for (int p = 0; p < kNearP; ++p) {
+                double y, z;
+                point64(p0 + p, qx[p], y, z);
+                if (!Pol::kLattice || p == 0) {
+                    qy[Pol::kLattice ? 0 : p] = y;
+                    qz[Pol::kLattice ? 0 : p] = z;
+                }
+                nacc[p] = 0.0;
+            }
+            // atoms inside the cutoff for every point of the warp: no test
+            for (int q = 0; q < n_ni; ++q) {
                 const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
-                const double dy = qy[0] - a.y, dz = qz[0] - a.z;
-                const double yz = fma(dz, dz, dy * dy);
+                if (Pol::kLattice) {
+                    // a lattice lane's points share y and z: dy^2 + dz^2 once per atom
+                    const double dy = qy[0] - a.y, dz = qz[0] - a.z;
+                    const double yz = fma(dz, dz, dy * dy);
 #pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    const double dx = qx[p] - a.x;
-                    const double u = __drcp_rn(fmax(fma(dx, dx, yz), cc.r2min));
-                    const double u3 = u * u * u;
-                    nacc[p] += u3 * fma(a.c12, u3, -a.c6);
+                    for (int p = 0; p < kNearP; ++p)
+                        nacc[p] += near_term64(qx[p] - a.x, yz, a.c12, a.c6, cc.r2min);
+                } else {
+#pragma unroll
+                    for (int p = 0; p < kNearP; ++p) {
+                        const double dy = qy[p] - a.y, dz = qz[p] - a.z;
+                        nacc[p] += near_term64(qx[p] - a.x, fma(dz, dz, dy * dy), a.c12, a.c6,
+                                               cc.r2min);
+                    }
                 }
             }
-        } else {
-            for (int q = 0; q < n_near; ++q) {
-                const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
-#pragma unroll
-                for (int p = 0; p < P; ++p) nacc[p] += pair64(a, qx[p], qy[p], qz[p], cc.r2min);
+            // atoms crossing the cutoff inside the warp box (boxes wider than
+            // rc - kNearR: coarse grids, sparse Widom bins): the cutoff decided per
+            // pair on the FP64 r^2. It differs from the reference's FP64 r^2 (cell
+            // frame, its own rounding) by far less than 1e-12 rc^2, so outside that
+            // window both decide alike and inside it exact_in_cutoff decides.
+            const double rc2lo = fw.rc2 * (1.0 - 1e-12), rc2hi = fw.rc2 * (1.0 + 1e-12);
+            for (int q = 0; q < n_ns; ++q) {
+                const int gid = s.cid[wn[kNearCap - 1 - q] >> 5];
+                const Atom64 a = atom64(fw, gid, o0, o1, o2);
+#pragma unroll 1
+                for (int p = 0; p < kNearP; ++p) {
+                    if (!(L.vmask & (1u << (p0 + p)))) continue;  // never stored
+                    const double dy = qy[Pol::kLattice ? 0 : p] - a.y;
+                    const double dz = qz[Pol::kLattice ? 0 : p] - a.z;
+                    const double dx = qx[p] - a.x;
+                    const double r2 = fmax(fma(dx, dx, fma(dz, dz, dy * dy)), cc.r2min);
+                    bool inside = r2 < rc2lo;
+                    if (!inside && r2 < rc2hi) {
+                        double f[3];
+                        pol.point(w, lane, p0 + p, f);
+                        inside = exact_in_cutoff(fw, f, gid, cc.r2min);
+                    }
+                    if (inside) {
+                        const double u = rcp64_nr(r2);
+                        const double u3 = u * u * u;
+                        nacc[p] += u3 * fma(a.c12, u3, -a.c6);
+                    }
+                }
             }
-        }
 #pragma unroll
-        for (int p = 0; p < P; ++p) tot_at(s, p) += nacc[p];
+            for (int p = 0; p < kNearP; ++p) tot_at(s, p0 + p) += nacc[p];
+        }
     }
 }
 

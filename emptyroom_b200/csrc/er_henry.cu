@@ -494,7 +494,7 @@ int henry_one(er_ctx* ctx, HenryPipe& P, const FwRecord& fw, double temperature,
             return set_error(ctx, ER_ERR_NOMEM, "henry batch: grid/mask allocation failed");
         GridTask t;
         int s = fill_grid_task(ctx, fw, bd[0], bd[1], bd[2], (float*)P.grid.ptr, t, 4);
-        if (s == ER_OK) s = launch_grid_plain_on(ctx, t, PREC_COMP, st);
+        if (s == ER_OK) s = launch_grid_plain_on(ctx, t, PREC_NEAR64, st);
         if (s == ER_OK)
             s = block_pockets_device_on(ctx, P.ps, st, (const float*)P.grid.ptr, bd[0], bd[1],
                                         bd[2], temperature, (uint8_t*)P.mask.ptr, &npk);

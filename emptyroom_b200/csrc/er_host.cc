@@ -212,6 +212,7 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
     f.img_xyz.resize(n);
     f.img_par.resize(2 * n);
     f.img_id.resize(n);
+    f.img_lj64.resize(2 * n);
     std::vector<int> fill(count.begin(), count.end() - 1);
     for (size_t q = 0; q < n; ++q) {
         const int dst = fill[cell[q]]++;
@@ -219,6 +220,9 @@ int build_framework(const er_framework_desc& d, double h, HostFramework& f, std:
         f.img_par[2 * dst] = par[2 * q];
         f.img_par[2 * dst + 1] = par[2 * q + 1];
         f.img_id[dst] = ids[q];
+        const size_t a = ids[q] / (uint32_t)ipa;
+        f.img_lj64[2 * dst] = f.atom_lj64[2 * a];
+        f.img_lj64[2 * dst + 1] = f.atom_lj64[2 * a + 1];
     }
     return ER_OK;
 }

@@ -30,6 +30,7 @@ struct HostFramework {
     std::vector<int> cell_start;        // nc0*nc1*nc2 + 1
     std::vector<HostImage> atom_frac;   // x_f, y_f, z_f, sig2 per atom
     std::vector<double> atom_lj64;      // 2 per atom: C12, C6 in FP64
+    std::vector<double> img_lj64;       // 2 per image: its atom's C12, C6 in FP64
 };
 
 // Validates desc and fills everything of `out` but the image cell list

@@ -19,7 +19,8 @@ struct FwDev {
     const uint32_t* img_id;   // atom * imgs_per_atom + image code
     const int* cell_start;    // nc0*nc1*nc2 + 1 offsets into the image arrays
     const double4* atom_frac; // FP64 fractional (x_f, y_f, z_f, sig2) per atom
-    const double2* atom_lj64; // FP64 (C12, C6) per atom (near pairs of PREC_NEAR64)
+    const double2* atom_lj64; // FP64 (C12, C6) per atom
+    const double2* img_lj64;  // FP64 (C12, C6) per image (near pairs of PREC_NEAR64)
     int n_img;
     int n_atoms;
     int nc[3];                // cells per axis

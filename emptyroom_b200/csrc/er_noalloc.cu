@@ -7,12 +7,13 @@
 // cudaMalloc / cudaFree may bring. They still want the insertion-averaged
 // Boltzmann factor of energies they already hold on the device. This entry
 // point reduces such an energy array with the same FP64 log-sum-exp tree as
-// er_henry, and keeps its only scratch -- one partial (m, s, se, count) per
-// reduction block plus the final one, 4097 x 32 bytes -- in a file-scope
-// static device array that every GPU loading this library holds until the
-// process exits. Each call writes every slot it later reads, so nothing has
-// to be cleared between calls; two calls that run at the same time on one
-// GPU share the array and race.
+// er_henry, and keeps its only scratch -- one partial (m, s, se, n_inf,
+// n_bad) per reduction block plus the final one, 4097 x 40 bytes -- in a
+// file-scope static device array that every GPU loading this library holds
+// until the process exits. Each call writes every slot it later reads, so
+// nothing has to be cleared between calls; two calls that run at the same
+// time on one GPU share the array and race. Index arithmetic is 64-bit, so
+// every n up to ER_HENRY_STATS_NOALLOC_MAX_N partitions without overflow.
 #include <math.h>
 
 #include <algorithm>
@@ -27,6 +28,7 @@ namespace noalloc {
 struct Stats {
     double m, s, se;
     double n_inf;  // energies equal to +inf (weight 0), e.g. blocked insertions
+    double n_bad;  // NaN or -inf energies: no defined weight, the call fails
 };
 
 // Reduction blocks; the static array holds kSlots partials plus the result.
@@ -35,12 +37,12 @@ constexpr int kSlots = 4096;
 static __device__ __align__(256) Stats g_scratch[kSlots + 1];
 
 __device__ __forceinline__ Stats merge(Stats a, Stats b) {
-    const double ninf = a.n_inf + b.n_inf;
-    if (b.s == 0.0) return Stats{a.m, a.s, a.se, ninf};
-    if (a.s == 0.0) return Stats{b.m, b.s, b.se, ninf};
+    const double ninf = a.n_inf + b.n_inf, nbad = a.n_bad + b.n_bad;
+    if (b.s == 0.0) return Stats{a.m, a.s, a.se, ninf, nbad};
+    if (a.s == 0.0) return Stats{b.m, b.s, b.se, ninf, nbad};
     const double M = fmax(a.m, b.m);
     const double fa = exp(a.m - M), fb = exp(b.m - M);
-    return Stats{M, a.s * fa + b.s * fb, a.se * fa + b.se * fb, ninf};
+    return Stats{M, a.s * fa + b.s * fb, a.se * fa + b.se * fb, ninf, nbad};
 }
 
 __device__ __forceinline__ Stats tree(Stats v, Stats* sm) {
@@ -56,16 +58,21 @@ __device__ __forceinline__ Stats tree(Stats v, Stats* sm) {
 
 // Block b reduces energies [b*chunk, (b+1)*chunk) in a fixed order and writes
 // its triple to scratch[b]; every slot it will read later is written first.
-__global__ void __launch_bounds__(256) partial_kernel(const float* __restrict__ E, int n,
-                                                      double T, int chunk,
+__global__ void __launch_bounds__(256) partial_kernel(const float* __restrict__ E, int64_t n,
+                                                      double T, int64_t chunk,
                                                       Stats* __restrict__ scratch) {
     __shared__ Stats sm[256];
-    const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
-    Stats acc{-INFINITY, 0.0, 0.0, 0.0};
-    for (int i = lo + threadIdx.x; i < hi; i += 256) {
+    const int64_t lo = (int64_t)blockIdx.x * chunk;
+    const int64_t hi = lo + chunk < n ? lo + chunk : n;
+    Stats acc{-INFINITY, 0.0, 0.0, 0.0, 0.0};
+    for (int64_t i = lo + threadIdx.x; i < hi; i += 256) {
         const float ef = E[i];
-        if (isinf(ef)) {  // an infinite energy has weight 0
+        if (ef == INFINITY) {  // +inf (a blocked insertion) has weight 0
             acc.n_inf += 1.0;
+            continue;
+        }
+        if (isnan(ef) || ef == -INFINITY) {  // no defined weight
+            acc.n_bad += 1.0;
             continue;
         }
         const double e = (double)ef;
@@ -87,7 +94,7 @@ __global__ void __launch_bounds__(256) partial_kernel(const float* __restrict__ 
 
 __global__ void __launch_bounds__(256) final_kernel(Stats* __restrict__ scratch, int nb) {
     __shared__ Stats sm[256];
-    Stats acc{-INFINITY, 0.0, 0.0, 0.0};
+    Stats acc{-INFINITY, 0.0, 0.0, 0.0, 0.0};
     for (int i = threadIdx.x; i < nb; i += 256) acc = merge(acc, scratch[i]);
     const Stats r = tree(acc, sm);
     if (threadIdx.x == 0) scratch[kSlots] = r;
@@ -135,12 +142,12 @@ extern "C" int er_henry_stats_noalloc(er_ctx* ctx, const float* energies, int64_
     noalloc::Stats* scratch = nullptr;
     int st = noalloc::scratch_for(ctx, &scratch);
     if (st != ER_OK) return st;
-    const int ni = (int)n;
-    // the same block partition as er_henry's reduction (4 blocks per SM, at most kSlots)
-    const int rblocks = std::min(noalloc::kSlots, std::max(1, ctx->num_sms * 4));
-    const int chunk = (ni + rblocks - 1) / rblocks;
-    const int nrb = (ni + chunk - 1) / chunk;
-    noalloc::partial_kernel<<<nrb, 256, 0, ctx->stream>>>(energies, ni, temperature, chunk,
+    // the block partition of er_henry's reduction (4 blocks per SM, at most
+    // kSlots), computed in 64-bit so that it cannot overflow at the top of the range
+    const int64_t rblocks = std::min<int64_t>(noalloc::kSlots, std::max(1, ctx->num_sms * 4));
+    const int64_t chunk = (n + rblocks - 1) / rblocks;
+    const int nrb = (int)((n + chunk - 1) / chunk);
+    noalloc::partial_kernel<<<nrb, 256, 0, ctx->stream>>>(energies, n, temperature, chunk,
                                                            scratch);
     noalloc::final_kernel<<<1, 256, 0, ctx->stream>>>(scratch, nrb);
     ER_CUDA(ctx, cudaGetLastError());
@@ -148,6 +155,10 @@ extern "C" int er_henry_stats_noalloc(er_ctx* ctx, const float* energies, int64_
     ER_CUDA(ctx, cudaMemcpyAsync(&r, scratch + noalloc::kSlots, sizeof(r), cudaMemcpyDeviceToHost,
                                  ctx->stream));
     ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (r.n_bad > 0.0)
+        return set_error(ctx, ER_ERR_INVALID,
+                         "henry_stats_noalloc: " + std::to_string((long long)r.n_bad) +
+                             " energies are NaN or -inf");
     out->log_scale = r.m;
     out->sum_w_scaled = r.s;
     out->sum_ew_scaled = r.se;

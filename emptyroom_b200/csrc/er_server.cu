@@ -318,7 +318,7 @@ struct er_server {
             } else {
                 er::GridTask t;
                 st = er::fill_grid_task(ctx, *fr, job.nx, job.ny, job.nz, g.ptr, t);
-                if (st == ER_OK) st = er::launch_grid_plain_on(ctx, t, er::PREC_COMP, sl.stream);
+                if (st == ER_OK) st = er::launch_grid_plain_on(ctx, t, er::PREC_NEAR64, sl.stream);
                 if (st == ER_OK && job.grid_out_host &&
                     cudaMemcpyAsync(job.grid_out_host, g.ptr, g.bytes, cudaMemcpyDeviceToHost,
                                     sl.stream) != cudaSuccess) {

@@ -90,9 +90,15 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);
 #define ER_OUT_DEVICE 0x1    /* out is a device pointer on the context's device */
 #define ER_OUT_F32 0x0       /* float per point */
 #define ER_OUT_F64 0x2       /* double per point (the reference's sheet type) */
-#define ER_PREC_COMP 0x0     /* FP32 pair terms, compensated (two-float) accumulation */
-#define ER_PREC_NEAR64 0x08  /* as ER_PREC_COMP, with the pairs of atoms within 5 A of
-                                a warp's points in FP64 (the default of er_henry) */
+#define ER_PREC_NEAR64 0x0  /* default: FP32 pair terms except the pairs of atoms within
+                                5 A of a warp's points, which are FP64 (the large terms
+                                whose FP32 rounding dominates where terms cancel); FP32
+                                sums of 64 terms folded into FP64 per-point totals.
+                                Within 1e-5 relative of FP64 on points with E < -10 K */
+#define ER_PREC_COMP 0x08    /* all pair terms FP32, FP32 sums of 64 terms folded into
+                                FP64 per-point totals: faster, but its error on E < 0
+                                points reaches ~2e-5 relative where large near terms
+                                cancel */
 #define ER_PREC_FP32 0x10    /* FP32 pair terms, plain FP32 accumulation */
 #define ER_PREC_FP64 0x20    /* FP64 pair terms and accumulation, same pair set as the
                                 FP32 modes (precision sweeps); needs ER_OUT_F64 */
@@ -138,12 +144,14 @@ typedef struct {
                                    first job of its class (atom density, grid spacing,
                                    cutoff); choices are cached in the context. A job's
                                    result then equals er_grid with that variant's flag. */
-#define ER_BATCH_NEAR64 0x400 /* or-ed into mode: the ER_PREC_NEAR64 pair sum (pairs of
-                                 atoms within 5 A of a warp's points in FP64) instead of
-                                 ER_PREC_COMP; results equal er_grid with ER_PREC_NEAR64 */
+#define ER_BATCH_COMP 0x400 /* or-ed into mode: the ER_PREC_COMP pair sum (all pair terms
+                               FP32) instead of the default ER_PREC_NEAR64; results then
+                               equal er_grid with ER_PREC_COMP */
 
 /* Runs many grid jobs (uneven frameworks, probes, grid sizes). Results are
- * identical between the two modes and independent of the job mix. */
+ * identical between the two modes and independent of the job mix; each job
+ * equals er_grid of the same framework and dims with the same precision flag
+ * (and ER_TILE_P8 where the plan picked that variant). */
 int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode);
 
 /* A batch plan fixes the work queue once and replays it as a CUDA graph. */
@@ -186,8 +194,8 @@ int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t
 /* Widom insertions for n frameworks: the henry tool's per-structure run
  * (src/henry.cu:63-174, one structure per process there) for many structures
  * in one call. For entry k: when the blocking dims are non-zero (each >= 2),
- * the FP32 energy grid of block_nx x block_ny x block_nz points (as er_grid,
- * ER_PREC_COMP), its pocket mask (as er_block_pockets_device, pocketblocking.cc:
+ * the FP32 energy grid of block_nx x block_ny x block_nz points (as er_grid
+ * with default flags), its pocket mask (as er_block_pockets_device, pocketblocking.cc:
  * 126-391) and er_henry of fw_ids[k] with seed seeds[k] and that mask; with
  * all three dims 0, er_henry alone. The frameworks run on up to three
  * concurrent pipelines (a stream, scratch and a host thread each, kept by the
@@ -204,13 +212,17 @@ int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
  * For callers that cannot call cudaMalloc -- a code that reserves all of its
  * device memory up front in its own pool, or a loop that cannot take the
  * implicit synchronisation and unbounded latency of cudaMalloc/cudaFree.
- * energies: device float[n] (an entry of +inf has weight 0 and is counted in
- * n_blocked); result as er_henry's reduction (FP64 log-sum-exp, same block
- * partition) with n_insertions = n. Its scratch is one file-scope static
- * device array of 4097 x 32 bytes, held by every GPU that loads this library
- * until the process exits; the first call on a device looks up that array's
- * address, so make it before any stream capture. Calls that overlap on one
- * GPU share the array and race. n above ER_HENRY_STATS_NOALLOC_MAX_N is
+ * energies: device float[n]. An entry of +inf has weight 0 and is counted in
+ * n_blocked; a NaN or -inf entry has no defined weight and makes the call
+ * return ER_ERR_INVALID. The result is er_henry's reduction (FP64
+ * log-sum-exp, the same block partition) with n_insertions = n. Its scratch
+ * is one file-scope static device array of 4097 x 40 bytes, held by every GPU
+ * that loads this library until the process exits. The first call on a
+ * device looks up that array's address (cudaGetSymbolAddress) with the
+ * device current; make that first call before any stream capture begins.
+ * The call is synchronous: it returns once the result has reached the host.
+ * Calls that overlap on one GPU (from several host threads or contexts)
+ * share the array and race. n outside [1, ER_HENRY_STATS_NOALLOC_MAX_N] is
  * rejected with ER_ERR_LIMIT. */
 #define ER_HENRY_STATS_NOALLOC_MAX_N 2147483647LL
 int er_henry_stats_noalloc(er_ctx* ctx, const float* energies, int64_t n, double temperature,

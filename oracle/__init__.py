@@ -75,6 +75,26 @@ def lib():
         L.oracle_grid_interp.restype = None
         L.oracle_grid_interp.argtypes = [_dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp,
                                          ctypes.c_int64, _dp]
+        L.oracle_points_cells.restype = ctypes.c_int
+        L.oracle_points_cells.argtypes = [_dp, ctypes.c_int, _dp, _ip, ctypes.c_double,
+                                          ctypes.c_double, _dp, ctypes.c_int64, _dp, _dp, _dp,
+                                          ctypes.c_int]
+        L.oracle_grid_cells.restype = ctypes.c_int
+        L.oracle_grid_cells.argtypes = [_dp, ctypes.c_int, _dp, _ip, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                        ctypes.c_int]
+        L.oracle_henry_cells.restype = ctypes.c_int
+        L.oracle_henry_cells.argtypes = [_dp, ctypes.c_int, _dp, _ip, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, _u8p,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                         ctypes.c_int]
+        L.oracle_cell_matrices.restype = ctypes.c_int
+        L.oracle_cell_matrices.argtypes = [ctypes.c_double] * 6 + [_dp, _dp, _dp]
+        L.oracle_replication_factors.restype = ctypes.c_int
+        L.oracle_replication_factors.argtypes = [_dp, ctypes.c_double, ctypes.c_int, _ip]
+        L.oracle_synth_positions.restype = ctypes.c_int
+        L.oracle_synth_positions.argtypes = [ctypes.c_uint64, _dp, ctypes.c_int, ctypes.c_double,
+                                             _dp]
         _lib = L
     return _lib
 
@@ -222,6 +242,90 @@ def henry(particles, t, rep, rc2, T, seed, n_ins, mask=None, want_energies=False
     if en is not None:
         res["energies"] = en
     return res
+
+
+# ------------------------------------------------ cell-list form of the sums
+def points_cells(particles, t, rep, rc2, pts, min_r=1e-12, n_threads=0):
+    """(energy, sum |term|, in-cutoff count) per point: the terms of `points`
+    summed cell by cell (er_oracle_cells.c)."""
+    p, tm, r = _prep(particles, t, rep)
+    q = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    e = np.empty(len(q)); s = np.empty(len(q)); c = np.empty(len(q))
+    st = lib().oracle_points_cells(_ptr(p, _dp), len(p), _ptr(tm, _dp), _ptr(r, _ip),
+                                   float(rc2), float(min_r), _ptr(q, _dp), len(q), _ptr(e, _dp),
+                                   _ptr(s, _dp), _ptr(c, _dp), int(n_threads))
+    if st:
+        raise MemoryError("oracle_points_cells")
+    return e, s, c
+
+
+def grid_cells(particles, t, rep, rc2, dims, n_threads=0, want_abs=False):
+    """FP64 grid (and sum |term| per point) by the cell-list sum."""
+    p, tm, r = _prep(particles, t, rep)
+    nx, ny, nz = (int(d) for d in dims)
+    e = np.empty(nx * ny * nz)
+    s = np.empty(nx * ny * nz) if want_abs else None
+    st = lib().oracle_grid_cells(_ptr(p, _dp), len(p), _ptr(tm, _dp), _ptr(r, _ip), float(rc2),
+                                 nx, ny, nz, _ptr(e, _dp), _ptr(s, _dp) if want_abs else None,
+                                 int(n_threads))
+    if st:
+        raise MemoryError("oracle_grid_cells")
+    e = e.reshape(nx, ny, nz)
+    return (e, s.reshape(nx, ny, nz)) if want_abs else e
+
+
+def henry_cells(particles, t, rep, rc2, T, seed, n_ins, mask=None, want_energies=False,
+                n_threads=0):
+    """`henry` with the cell-list energies; same result keys."""
+    p, tm, r = _prep(particles, t, rep)
+    out = np.zeros(5, dtype=np.float64)
+    en = np.empty(int(n_ins), dtype=np.float64) if want_energies else None
+    if mask is not None:
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        mnx, mny, mnz = m.shape
+        mp = _ptr(m, _u8p)
+    else:
+        mnx = mny = mnz = 0
+        mp = None
+    st = lib().oracle_henry_cells(_ptr(p, _dp), len(p), _ptr(tm, _dp), _ptr(r, _ip), float(rc2),
+                                  float(T), int(seed), int(n_ins), mp, mnx, mny, mnz,
+                                  _ptr(out, _dp), _ptr(en, _dp) if en is not None else None,
+                                  int(n_threads))
+    if st:
+        raise MemoryError("oracle_henry_cells")
+    res = dict(sum_w=out[0], sum_ew=out[1], n=out[2], max_neg_e_over_t=out[3],
+               n_blocked=int(out[4]))
+    if en is not None:
+        res["energies"] = en
+    return res
+
+
+# --------------------------------------------- generators of the workloads
+def cell_matrices(a, b, c, alpha, beta, gamma):
+    """(t_matrix 3x3, inv 3x3, volume), src/Framework.cc:113-142."""
+    t = np.zeros(9); inv = np.zeros(9); v = np.zeros(1)
+    if lib().oracle_cell_matrices(a, b, c, alpha, beta, gamma, _ptr(t, _dp), _ptr(inv, _dp),
+                                  _ptr(v, _dp)):
+        raise ValueError("degenerate cell")
+    return t.reshape(3, 3), inv.reshape(3, 3), float(v[0])
+
+
+def replication_factors(t, r_cutoff, factor=1):
+    tm = np.ascontiguousarray(t, dtype=np.float64).reshape(9)
+    rep = np.zeros(3, dtype=np.int32)
+    if lib().oracle_replication_factors(_ptr(tm, _dp), float(r_cutoff), int(factor),
+                                        _ptr(rep, _ip)):
+        raise ValueError("replication factors")
+    return tuple(int(x) for x in rep)
+
+
+def synth_positions(seed, t, n_atoms, d_min):
+    tm = np.ascontiguousarray(t, dtype=np.float64).reshape(9)
+    out = np.empty((int(n_atoms), 3))
+    if lib().oracle_synth_positions(int(seed), _ptr(tm, _dp), int(n_atoms), float(d_min),
+                                    _ptr(out, _dp)):
+        raise ValueError(f"could not place {n_atoms} atoms at d_min={d_min}")
+    return out
 
 
 def block_pockets(grid3, T):

@@ -341,7 +341,7 @@ void oracle_insertion_point(uint64_t seed, uint64_t i, double out[3]) {
 
 /* An insertion is blocked when any of the 8 corners of its grid cell is set.
  * Cell lookup follows src/gcmc.cc:155-157 (floor(x_f / dx_f), dx_f = 1/(N-1)). */
-static int insertion_blocked(const uint8_t* mask, int nx, int ny, int nz, const double p[3]) {
+int oracle_insertion_blocked(const uint8_t* mask, int nx, int ny, int nz, const double p[3]) {
     double dxf = 1.0 / (nx - 1), dyf = 1.0 / (ny - 1), dzf = 1.0 / (nz - 1);
     int i0 = (int)floor(p[0] / dxf), j0 = (int)floor(p[1] / dyf), k0 = (int)floor(p[2] / dzf);
     if (i0 > nx - 2) i0 = nx - 2;
@@ -367,7 +367,7 @@ static void* henry_worker(void* arg) {
     for (int64_t i = lo; i < hi; i++) {
         double p[3];
         oracle_insertion_point(jb->seed, (uint64_t)i, p);
-        if (jb->mask && insertion_blocked(jb->mask, jb->mnx, jb->mny, jb->mnz, p)) {
+        if (jb->mask && oracle_insertion_blocked(jb->mask, jb->mnx, jb->mny, jb->mnz, p)) {
             if (jb->energies) jb->energies[i] = INFINITY;
             nb += 1.0;
             continue;

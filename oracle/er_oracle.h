@@ -110,6 +110,36 @@ int oracle_block_pockets(double* grid, int nx, int ny, int nz, double temperatur
 void oracle_grid_interp(const double* grid, int nx, int ny, int nz, const double* pts,
                         int64_t n, double* out);
 
+/* An insertion is blocked when any of the 8 corners of its mask cell is set
+ * (cell lookup of src/gcmc.cc:155-157). */
+int oracle_insertion_blocked(const uint8_t* mask, int nx, int ny, int nz, const double p[3]);
+
+/* ---- er_oracle_cells.c: the same FP64 sums over a Cartesian cell list ----
+ * Every term and the set of terms equal the image loop's; only the order of
+ * the additions differs. Return 0, or -1 when memory ran out. */
+/* Per point (n x 3 fractional): energy, sum |term| and in-cutoff term count
+ * (each output may be NULL). */
+int oracle_points_cells(const or_particle* atoms, int n_atoms, const double t[9],
+                        const int rep[3], double rc2, double min_r, const double* pts,
+                        int64_t n_pts, double* energy, double* sum_abs, double* n_terms,
+                        int n_threads);
+/* Whole grid (axes i/(N-1), layout k + j nz + i ny nz); sum_abs may be NULL. */
+int oracle_grid_cells(const or_particle* atoms, int n_atoms, const double t[9], const int rep[3],
+                      double rc2, int nx, int ny, int nz, double* energy, double* sum_abs,
+                      int n_threads);
+/* oracle_henry with the cell-list energy (same points, mask test and output). */
+int oracle_henry_cells(const or_particle* atoms, int n_atoms, const double t[9],
+                       const int rep[3], double rc2, double T, uint64_t seed, int64_t n_ins,
+                       const uint8_t* mask, int mnx, int mny, int mnz, double* out,
+                       double* energies, int n_threads);
+
+/* ---- er_oracle_synth.c: the benchmark's seeded frameworks ---- */
+int oracle_cell_matrices(double a, double b, double c, double alpha_deg, double beta_deg,
+                         double gamma_deg, double t[9], double inv[9], double* volume);
+int oracle_replication_factors(const double t[9], double r_cutoff, int factor, int rep[3]);
+int oracle_synth_positions(uint64_t seed, const double t[9], int n_atoms, double d_min,
+                           double* frac);
+
 #ifdef __cplusplus
 }
 #endif

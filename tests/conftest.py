@@ -27,47 +27,56 @@ def ctx():
     c.close()
 
 
-# Tolerances of the CUDA grid against the FP64 reference. The CUDA path sums
-# FP32 pair terms (compensated accumulation, the exact FP64 cutoff set); each
-# term then carries a relative rounding error of order 1e-6 (FP32 positions
-# amplified up to 12x by r^-12), so the error of a sum is bounded by a
-# multiple of S = sum |term| (oracle.points_abs), not of |E|, where terms cancel:
-#   E_ref < 0         : |dE| <= RTOL_NEG * |E_ref| + STOL * S
-#   0 <= E_ref < 1e10 : |dE| <= RTOL_POS * |E_ref| + STOL * S   (repulsive wall)
-#   E_ref >= 1e30     : E == ER_ENERGY_CAP
-# Without S (large sampled cases) ATOL replaces STOL * S.
+# Tolerances of the CUDA grid against the FP64 reference. The default mode
+# (ER_PREC_NEAR64) sums FP32 pair terms, except the pairs of atoms within 5 A
+# of a warp's points, which are FP64, over the exact FP64 cutoff set:
+#   E_ref < -DELTA_NEG       : |dE| <= RTOL_NEG * |E_ref|   (1e-5 relative, no slack)
+#   -DELTA_NEG <= E_ref < 0  : |dE| <= RTOL_NEG * |E_ref| + STOL * S
+#   0 <= E_ref < 1e10        : |dE| <= RTOL_POS * |E_ref| + STOL * S   (repulsive wall)
+#   E_ref >= 1e30            : E == ER_ENERGY_CAP
+# S = sum |term| (oracle.points_abs). Near the zero crossing a relative error
+# is undefined (|E| -> 0 while the FP32 terms' rounding stays a multiple of
+# S), so only there does the bound scale with S. Without S (large sampled
+# cases) ATOL replaces STOL * S. The all-FP32 modes (ER_PREC_COMP,
+# ER_PREC_FP32) are checked with `loose=True`: the S-scaled bound on every
+# E < 0 point, since their FP32 near terms leave ~2e-7 S where terms cancel.
 RTOL_NEG = 1e-5
+DELTA_NEG = 10.0
 RTOL_POS = 1e-4
 STOL = 2e-6
 ATOL = 2e-3
 
 
-def grid_errors(e_gpu, e_ref, scale=None):
-    """Per-class error statistics used by the parity tests and the bench."""
+def grid_errors(e_gpu, e_ref, scale=None, loose=False):
+    """Per-class error statistics used by the parity tests."""
     e_gpu = np.asarray(e_gpu, dtype=np.float64).ravel()
     e_ref = np.asarray(e_ref, dtype=np.float64).ravel()
     d = np.abs(e_gpu - e_ref)
-    slack = ATOL if scale is None else STOL * np.asarray(scale, dtype=np.float64).ravel()
+    slack = (np.full(e_ref.shape, ATOL) if scale is None
+             else STOL * np.asarray(scale, dtype=np.float64).ravel())
     neg = e_ref < 0
+    deep = e_ref < -DELTA_NEG
+    shallow = neg & ~deep
     pos = (e_ref >= 0) & (e_ref < 1e10)
-    out = {"n": e_ref.size, "n_neg": int(neg.sum())}
-    s_neg = slack if np.isscalar(slack) else slack[neg]
-    s_pos = slack if np.isscalar(slack) else slack[pos]
+    out = {"n": e_ref.size, "n_neg": int(neg.sum()), "n_deep": int(deep.sum())}
     if neg.any():
         rel = d[neg] / np.abs(e_ref[neg])
         out["neg_max_rel"] = float(rel.max())
         out["neg_p99_rel"] = float(np.percentile(rel, 99))
         out["neg_max_abs"] = float(d[neg].max())
-        if not np.isscalar(slack):
-            out["neg_max_rel_scale"] = float((d[neg] / np.maximum(slack[neg] / STOL, 1e-300)).max())
-        out["neg_ok"] = bool(np.all(d[neg] <= RTOL_NEG * np.abs(e_ref[neg]) + s_neg))
+    if deep.any():
+        rel = d[deep] / np.abs(e_ref[deep])
+        out["deep_max_rel"] = float(rel.max())
+        out["deep_p99_rel"] = float(np.percentile(rel, 99))
+    if loose:
+        ok_neg = d[neg] <= RTOL_NEG * np.abs(e_ref[neg]) + slack[neg]
     else:
-        out["neg_ok"] = True
+        ok_neg = np.concatenate([d[deep] <= RTOL_NEG * np.abs(e_ref[deep]),
+                                 d[shallow] <= RTOL_NEG * np.abs(e_ref[shallow]) + slack[shallow]])
+    out["neg_ok"] = bool(np.all(ok_neg))
     if pos.any():
         out["pos_max_rel"] = float((d[pos] / np.maximum(np.abs(e_ref[pos]), 1.0)).max())
-        out["pos_ok"] = bool(np.all(d[pos] <= RTOL_POS * np.abs(e_ref[pos]) + s_pos))
-    else:
-        out["pos_ok"] = True
+    out["pos_ok"] = bool(np.all(d[pos] <= RTOL_POS * np.abs(e_ref[pos]) + slack[pos]))
     cap = e_ref >= 1e30
     out["cap_ok"] = bool(np.all(e_gpu[cap] == np.float32(1e30)))
     return out

@@ -114,3 +114,10 @@ def test_lorentz_berthelot_matches_reference_rule():
     e, s2 = er.lorentz_berthelot([30.0, 52.83], [3.12, 3.43], 148.0, 3.73)
     np.testing.assert_allclose(e, np.sqrt(148.0 * np.array([30.0, 52.83])), rtol=0)
     np.testing.assert_allclose(s2, ((3.73 + np.array([3.12, 3.43])) / 2.0) ** 2, rtol=0)
+
+
+def test_noalloc_limit_matches_header():
+    import re
+    hdr = open(os.path.join(ROOT, "include", "emptyroom_b200.h")).read()
+    m = re.search(r"#define ER_HENRY_STATS_NOALLOC_MAX_N (\d+)LL", hdr)
+    assert m and int(m.group(1)) == _capi.ER_HENRY_STATS_NOALLOC_MAX_N == 2**31 - 1

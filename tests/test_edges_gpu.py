@@ -49,7 +49,7 @@ def test_oversized_sheet_and_accessibility_refused(ctx):
 
 @pytest.mark.parametrize("mode", [er.ER_BATCH_PERSISTENT, er.ER_BATCH_PLAIN,
                                   er.ER_BATCH_PERSISTENT | er.ER_BATCH_HOST_OUT,
-                                  er.ER_BATCH_PERSISTENT | er.ER_BATCH_NEAR64])
+                                  er.ER_BATCH_PERSISTENT | er.ER_BATCH_COMP])
 def test_empty_batch_is_a_no_op(ctx, mode):
     ctx.grid_batch([], mode)
     plan = ctx.batch_plan([], mode & ~er.ER_BATCH_HOST_OUT)

@@ -114,3 +114,63 @@ def test_oracle_interp_matches_reference_live(seed):
     grid[rng.random(dims) < 0.05] = 1e13
     pts = rng.uniform(-3.0, 4.0, size=(3000, 3))
     assert np.array_equal(oracle.grid_interp(grid, pts), oracle.ref_grid_interp(grid, pts))
+
+
+# ---------------------------------------------------------- cell-list form
+def _cases():
+    from emptyroom_b200 import synth
+    return [synth.config1(0),
+            synth.make_framework(61, (9.1, 11.3, 8.7), (72, 104, 97), 60, probe="Xe"),
+            synth.make_framework(62, (21.0, 17.5, 26.0), (95, 80, 110), 700, probe="Kr")]
+
+
+@pytest.mark.parametrize("k", range(3))
+def test_cell_list_sum_equals_image_loop(k):
+    """er_oracle_cells.c sums the same terms as the image loop: identical term
+    counts, energies within a few ulps of sum |term| (only the order of the
+    additions differs)."""
+    f = _cases()[k]
+    P = f.particles()
+    pts = np.random.default_rng(k).random((400, 3))
+    for min_r in (1e-12, 1e-16):
+        e, s, c = oracle.points_cells(P, f.t_matrix, f.rep, f.rc2, pts, min_r)
+        ref = oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, min_r)
+        S = oracle.points_abs(P, f.t_matrix, f.rep, f.rc2, pts, min_r)
+        assert np.array_equal(c, oracle.points_pairs(P, f.t_matrix, f.rep, f.rc2, pts, min_r))
+        assert np.all(np.abs(e - ref) <= 1e-13 * S)
+        assert np.all(np.abs(s - S) <= 1e-13 * S)
+    dims = (7, 6, 9)
+    g = oracle.grid_cells(P, f.t_matrix, f.rep, f.rc2, dims)
+    g0 = oracle.grid(P, f.t_matrix, f.rep, f.rc2, dims)
+    S = oracle.grid_abs(P, f.t_matrix, f.rep, f.rc2, dims)
+    assert np.all(np.abs(g - g0) <= 1e-13 * S)
+
+
+def test_cell_list_henry_equals_image_loop():
+    from emptyroom_b200 import synth
+    f = synth.make_framework(63, (14.0, 15.0, 13.0), (90, 90, 90), 120, probe="Xe")
+    P = f.particles()
+    mask = (np.random.default_rng(2).random((9, 8, 10)) < 0.05).astype(np.uint8)
+    for m in (None, mask):
+        a = oracle.henry(P, f.t_matrix, f.rep, f.rc2, 298.0, 9, 3000, mask=m,
+                         want_energies=True)
+        b = oracle.henry_cells(P, f.t_matrix, f.rep, f.rc2, 298.0, 9, 3000, mask=m,
+                               want_energies=True)
+        assert a["n_blocked"] == b["n_blocked"]
+        assert abs(a["sum_w"] - b["sum_w"]) <= 1e-12 * a["sum_w"]
+        fin = np.isfinite(a["energies"])
+        assert np.array_equal(fin, np.isfinite(b["energies"]))
+
+
+def test_workload_generators_equal_the_library():
+    """The reference arm's frameworks (oracle/workloads.py) are the GPU arm's
+    (emptyroom_b200/synth.py) bit for bit."""
+    from emptyroom_b200 import synth
+    from oracle import workloads
+    for a, b in ((workloads.config2(256), synth.config2(256)),
+                 (workloads.config4(8), synth.config4(8))):
+        assert len(a) == len(b)
+        for x, y in zip(a, b):
+            assert np.array_equal(x.particles(), y.particles())
+            assert np.array_equal(x.t_matrix, y.t_matrix)
+            assert tuple(x.rep) == tuple(y.rep) and tuple(x.dims) == tuple(y.dims)

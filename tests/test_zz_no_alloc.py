@@ -58,3 +58,50 @@ def test_noalloc_rejects_out_of_range_sizes(ctx):
     st, _ = _noalloc(ctx, E.data_ptr(), (1 << 31), 298.0)
     assert st == 7
     assert b"ER_HENRY_STATS_NOALLOC_MAX_N" in _capi.lib().er_ctx_last_error(ctx.handle)
+
+
+def test_noalloc_blocked_and_undefined_energies(ctx):
+    """+inf entries (blocked insertions) have weight 0 and are counted; a NaN
+    or -inf entry has no defined Boltzmann weight and fails the call."""
+    import torch
+    T = 298.0
+    e = np.full(1000, -500.0, dtype=np.float32)
+    e[::7] = np.inf
+    E = torch.from_numpy(e).cuda()
+    st, got = _noalloc(ctx, E.data_ptr(), e.size, T)
+    assert st == 0
+    n_inf = int(np.isinf(e).sum())
+    assert got.n_blocked == n_inf
+    kh = (e.size - n_inf) * np.exp(500.0 / T) / e.size / T / 8.314
+    assert _close(got.kh_mol_m3_pa, kh)
+    for bad in (np.nan, -np.inf):
+        e2 = e.copy()
+        e2[3] = bad
+        E2 = torch.from_numpy(e2).cuda()
+        st, _ = _noalloc(ctx, E2.data_ptr(), e2.size, T)
+        assert st == 1  # ER_ERR_INVALID
+        assert b"NaN or -inf" in _capi.lib().er_ctx_last_error(ctx.handle)
+
+
+def test_noalloc_at_the_documented_maximum(ctx):
+    """n = ER_HENRY_STATS_NOALLOC_MAX_N (2^31 - 1 energies, 8.6 GB): with a
+    constant energy c every weight is exp(-c/T), so K_H = exp(-c/T)/(T 8.314)
+    and <E> = c in closed form; the block partition must not overflow."""
+    import torch
+    n = _capi.ER_HENRY_STATS_NOALLOC_MAX_N
+    c, T = -1234.5, 298.0
+    E = torch.full((n,), c, dtype=torch.float32, device="cuda")
+    # the fill runs on torch's stream, the library on its own non-blocking one
+    torch.cuda.synchronize()
+    try:
+        st, got = _noalloc(ctx, E.data_ptr(), n, T)
+        assert st == 0, _capi.lib().er_ctx_last_error(ctx.handle)
+        assert got.n_insertions == n and got.n_blocked == 0
+        kh = np.exp(-c / T) / T / 8.314
+        assert abs(got.kh_mol_m3_pa - kh) <= 1e-12 * kh
+        assert got.mean_energy == c
+        st, _ = _noalloc(ctx, E.data_ptr(), n + 1, T)
+        assert st == 7  # ER_ERR_LIMIT
+    finally:
+        del E
+        torch.cuda.empty_cache()
