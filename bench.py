@@ -4,20 +4,26 @@ Workload (one "step"): grids of 256 seeded triclinic frameworks (a, b, c in
 [8, 40] A, angles in [60, 120] deg, 100-5000 atoms log-uniform capped at 0.16
 atoms/A^3, 8 atom types, probes CH4 / Xe / Kr, grid spacing 0.1-0.2 A, cutoff
 12.5 A) computed by one persistent launch over a device work queue replayed
-as a CUDA graph. Data are synthetic (no dataset ships with the reference).
+as a CUDA graph, in the default precision mode (ER_PREC_NEAR64: FP32 pair
+terms, pairs of atoms within 5 A of a warp's points in FP64; within 1e-5
+relative of FP64 on E < -10 K points). Data are synthetic (no dataset ships
+with the reference).
 
-value   pair terms/s of the batched launch, inputs resident, device-timed with
-        CUDA events on the library's stream (in-cutoff pair terms counted
-        exactly by the same traversal in counting mode, outside the timing)
-e2e     the same metric through the C ABI with host buffers: per step every
-        framework is uploaded (host preparation + H2D), the batch runs, and
-        every grid is copied back to pinned host memory
+value    pair terms/s of the batched launch, inputs resident, device-timed with
+         CUDA events on the library's stream (in-cutoff pair terms counted
+         exactly by the same traversal in counting mode, outside the timing)
+e2e      the same metric through the C ABI with host buffers: per step every
+         framework is uploaded (host preparation + H2D), the batch runs, and
+         every grid is copied back to pinned host memory
 roofline pair terms/s x 11 FP32-pipe instructions per pair against the
-        device's FP32 FMA issue rate measured by er_probe_fp32_rate
+         device's FP32 FMA issue rate measured by er_probe_fp32_rate
+errors   the batch grids and the Widom K_H against the FP64 oracle: sampled
+         points of every grid, K_H of four Widom frameworks at full size
 cpu_baseline the reference's own ComputeGridSheet (oracle/_ref) on a bounded
-        sample of the same grids, on all host cores
+         sample of the same grids and of Widom insertion points, all host cores
 
-`--impl reference` times only the reference's CPU implementation.
+`--impl reference` times only the reference's CPU implementation (on
+frameworks built by oracle/workloads.py, without this library).
 Multi-GPU (torchrun): every rank runs its own 256-framework batch (weak
 scaling, no collective on the data path); timing is the max over ranks.
 """
@@ -38,6 +44,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "LJ pair terms/s & Widom insertions/s; served p50/p99 vs plain, same B200"
 PAIR_INSTR = 11  # FP32-pipe instructions credited per in-cutoff pair term
+WORKLOAD = "256-framework batched LJ grids (config 2)"
+DEEP = -10.0     # K: below this the grid tolerance is 1e-5 relative
 
 
 def dist_setup():
@@ -135,13 +143,13 @@ def upload_all(ctx, fws):
     return ctx.upload_many([(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws])
 
 
-def count_pairs(ctx, ups, fws):
-    """Exact in-cutoff pair terms per framework (counting traversal)."""
+def count_pairs(ctx, ups, dims_list):
+    """Exact in-cutoff pair terms per job (counting traversal)."""
     import torch
     counts = []
-    for u, f in zip(ups, fws):
-        buf = torch.empty(f.dims, dtype=torch.float32, device="cuda")
-        ctx.count_pairs_device(u, f.dims, buf.data_ptr())
+    for u, dims in zip(ups, dims_list):
+        buf = torch.empty(dims, dtype=torch.float32, device="cuda")
+        ctx.count_pairs_device(u, dims, buf.data_ptr())
         ctx.synchronize()
         counts.append(int(buf.double().sum().item()))
         del buf
@@ -172,57 +180,146 @@ def time_plan(ctx, plan, steps, warmup, l2buf):
     return times
 
 
-def cpu_baseline(fws, counts_fn, target_s=12.0):
-    """The reference's ComputeGridSheet on whole x-sheets of a few frameworks,
-    all host cores; returns pair terms/s on that sample."""
+def ref_grid_sample(fws, target_s, rng, cores, chunk=256):
+    """The reference's ComputeGridSheet (oracle/_ref; the oracle's image loop
+    when the reference was not built here), called on one-point axes, at
+    random grid points of frameworks drawn by grid size until target_s seconds
+    of work: (pair terms, seconds, samples). Each point costs the reference
+    what it costs inside a whole sheet (every image of every atom); the pair
+    terms of the sample are counted by the cell-list oracle."""
     import oracle
-    cores = os.cpu_count() or 1
     use_ref = oracle.ref_available()
-    rng = np.random.default_rng(7)
-    order = rng.permutation(len(fws))
-    done_pairs = 0.0
-    done_s = 0.0
+    pairs = secs = 0.0
     sample = []
-    for k in order:
-        f = fws[int(k)]
-        nx = f.dims[0]
-        sh = [int(rng.integers(0, nx))]
+    # frameworks drawn in proportion to their grid points: the sample's pair
+    # terms per second then estimate the whole batch's, whose frameworks cost
+    # the reference anything from a few hundred to ~1e6 image evaluations per point
+    w = np.array([float(np.prod(f.dims)) for f in fws])
+    w /= w.sum()
+    while secs < target_s:
+        k = int(rng.choice(len(fws), p=w))
+        f = fws[k]
         P = f.particles()
+        dims = np.array(f.dims)
+        pts = rng.integers(0, dims, size=(chunk, 3)) / (dims - 1.0)
         t0 = time.perf_counter()
         if use_ref:
-            oracle.ref_grid_sheets(P, f.t_matrix, f.rep, f.rc2, f.dims, sh, n_threads=cores)
+            oracle.ref_points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
         else:
-            ny, nz = f.dims[1], f.dims[2]
-            jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
-            pts = np.stack([np.full(jj.size, sh[0] / (nx - 1)), jj.ravel() / (ny - 1),
-                            kk.ravel() / (nz - 1)], -1)
             oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
-        dt = time.perf_counter() - t0
-        done_pairs += counts_fn(int(k), sh[0])
-        done_s += dt
-        sample.append(f"fw{int(k)}:x{sh[0]}")
-        if done_s >= target_s:
-            break
-    return {"value": done_pairs / done_s, "unit": "pair-terms/s", "cores": cores,
-            "kind": "reference" if use_ref else "port",
-            "sample": f"{len(sample)} whole x-sheets of {len(sample)} frameworks of the batch "
-                      f"({done_pairs:.3g} pair terms in {done_s:.1f} s)"}
+        secs += time.perf_counter() - t0
+        pairs += float(oracle.points_cells(P, f.t_matrix, f.rep, f.rc2, pts,
+                                           n_threads=cores)[2].sum())
+        sample.append(f"fw{k}")
+    return pairs, secs, sample
 
 
-def cpu_config1_grid():
-    """The reference's ComputeGridSheet on the whole config-1 32^3 grid, all
-    host cores (seconds)."""
+def ref_widom_sample(f, target_s, cores, seed=0):
+    """The reference's LJ routine (ComputeGridSheet at one-point axes, the sum
+    of src/doHenry.h:70-98) at the first Philox insertion points of stream
+    `seed`, plus exp(-E/T) accumulation, until target_s seconds: (insertions,
+    pair terms, seconds)."""
     import oracle
-    from emptyroom_b200 import synth
-    f = synth.config1(0)
+    use_ref = oracle.ref_available()
     P = f.particles()
+    n_done = 0
+    pairs = secs = 0.0
+    chunk = 2048
+    while secs < target_s:
+        pts = oracle.insertion_points(seed, chunk, n_done)
+        t0 = time.perf_counter()
+        if use_ref:
+            e = oracle.ref_points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
+        else:
+            e = oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, 1e-16, n_threads=cores)
+        np.exp(-e / 298.0).sum()
+        secs += time.perf_counter() - t0
+        pairs += float(oracle.points_cells(P, f.t_matrix, f.rep, f.rc2, pts, 1e-16,
+                                           n_threads=cores)[2].sum())
+        n_done += chunk
+        chunk = min(chunk * 2, 65536)
+    return n_done, pairs, secs
+
+
+def cpu_baseline(fws, fw_widom, target_s=10.0):
+    """The reference's own CPU code (oracle/_ref) on all host cores: whole
+    x-sheets of the batch's grids, and Widom insertion points of a config-4
+    framework; each leg a bounded sample extrapolated per pair term."""
+    import oracle
     cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    if oracle.ref_available():
-        oracle.ref_grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
-    else:
-        oracle.grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
-    return time.perf_counter() - t0
+    rng = np.random.default_rng(7)
+    pairs, secs, sample = ref_grid_sample(fws, target_s, rng, cores)
+    n_ins, wpairs, wsecs = ref_widom_sample(fw_widom, target_s * 0.6, cores)
+    return {"value": pairs / secs, "unit": "pair-terms/s", "cores": cores,
+            "kind": "reference" if oracle.ref_available() else "port",
+            "sample": f"{256 * len(sample)} random grid points of {len(sample)} randomly "
+                      f"chosen batch frameworks ({pairs:.3g} pair terms in {secs:.1f} s)",
+            "widom": {"insertions_per_s": n_ins / wsecs, "pair_terms_per_s": wpairs / wsecs,
+                      "sample": f"first {n_ins} Philox insertions of a config-4 cell (Xe) "
+                                f"in {wsecs:.1f} s, extrapolated per insertion"}}
+
+
+def grid_errors_block(fws, outs, cores, seed=11, n_deep=192, n_shallow=32, n_uniform=64):
+    """Error of every batch grid against the FP64 oracle (cell-list form) on
+    sampled points: up to n_deep points with E < -10 K, n_shallow with
+    -10 K <= E < 0 and n_uniform anywhere, chosen from the GPU grid."""
+    import torch
+
+    import oracle
+    rng = np.random.default_rng(seed)
+    deep_max, deep_p99, n_deep_pts = [], [], []
+    all_deep_rel, shallow_ratio, pos_rel = [], [], []
+    cap_ok = True
+    for f, o in zip(fws, outs):
+        flat = o.reshape(-1)
+        picks = []
+        for sel, cnt in ((flat < DEEP, n_deep), ((flat >= DEEP) & (flat < 0), n_shallow)):
+            idx = torch.nonzero(sel).reshape(-1)
+            if idx.numel():
+                take = torch.from_numpy(rng.choice(idx.numel(), size=min(cnt, idx.numel()),
+                                                   replace=False)).to(idx.device)
+                picks.append(idx[take].cpu().numpy())
+        picks.append(rng.integers(0, flat.numel(), size=n_uniform))
+        idx = np.unique(np.concatenate(picks))
+        got = flat[torch.from_numpy(idx).to(flat.device)].double().cpu().numpy()
+        dims = np.array(f.dims)
+        ijk = np.stack(np.unravel_index(idx, f.dims), -1)
+        pts = ijk / (dims - 1.0)
+        ref, S, _ = oracle.points_cells(f.particles(), f.t_matrix, f.rep, f.rc2, pts, 1e-12,
+                                        n_threads=cores)
+        d = np.abs(got - ref)
+        deep = ref < DEEP
+        shallow = (ref >= DEEP) & (ref < 0)
+        pos = (ref >= 0) & (ref < 1e10)
+        rel = d[deep] / np.abs(ref[deep])
+        n_deep_pts.append(int(deep.sum()))
+        deep_max.append(float(rel.max()) if rel.size else None)
+        deep_p99.append(float(np.percentile(rel, 99)) if rel.size else None)
+        all_deep_rel.append(rel)
+        if shallow.any():  # |dE| against 1e-5 |E| + 2e-6 S, the bound of the tests
+            shallow_ratio.append(float((d[shallow] / (1e-5 * np.abs(ref[shallow]) +
+                                                      2e-6 * S[shallow])).max()))
+        if pos.any():
+            pos_rel.append(float((d[pos] / np.maximum(np.abs(ref[pos]), 1.0)).max()))
+        cap = ref >= 1e30
+        cap_ok &= bool(np.all(got[cap] == np.float32(1e30)))
+    rel = np.concatenate(all_deep_rel)
+    return {"workload": f"all {len(fws)} batch grids (default mode), points sampled from each "
+                        f"grid: <= {n_deep} with E < {DEEP:g} K, <= {n_shallow} with "
+                        f"{DEEP:g} K <= E < 0, {n_uniform} uniform; FP64 oracle (cell-list "
+                        f"sum of the reference's terms)",
+            "deep": {"points": int(rel.size), "max_rel": float(rel.max()),
+                     "p99_rel": float(np.percentile(rel, 99)),
+                     "n_over_1e-5": int((rel > 1e-5).sum()),
+                     "grids_with_points": int(sum(1 for n in n_deep_pts if n))},
+            "shallow_max_over_bound": max(shallow_ratio) if shallow_ratio else None,
+            "pos_max_rel": max(pos_rel) if pos_rel else None,
+            "cap_ok": cap_ok,
+            "per_grid_deep_max_rel": [None if v is None else float(f"{v:.3g}")
+                                      for v in deep_max],
+            "per_grid_deep_p99_rel": [None if v is None else float(f"{v:.3g}")
+                                      for v in deep_p99],
+            "per_grid_deep_points": n_deep_pts}
 
 
 def run_ours(args, ws, rank, local, pg):
@@ -233,13 +330,13 @@ def run_ours(args, ws, rank, local, pg):
     ctx = er.Context(local)
     fws = make_workload(rank, args.frameworks)
     ups = upload_all(ctx, fws)
-    counts = count_pairs(ctx, ups, fws)
+    counts = count_pairs(ctx, ups, [f.dims for f in fws])
     pairs_step = float(sum(counts))
     points_step = float(sum(int(np.prod(f.dims)) for f in fws))
     outs = [torch.empty(f.dims, dtype=torch.float32, device="cuda") for f in fws]
     jobs = [(u, f.dims, o.data_ptr()) for u, f, o in zip(ups, fws, outs)]
-    # one persistent launch; the kernel variant of each job class picked by
-    # the autotuner (timed at plan creation, outside the timed region)
+    # one persistent launch in the default (NEAR64) mode; the kernel variant of
+    # each job class picked by the autotuner at plan creation, outside the timing
     plan = ctx.batch_plan(jobs, er.ER_BATCH_PERSISTENT | er.ER_BATCH_AUTOTUNE)
     tiles = [plan.tile(k) for k in range(len(jobs))]
     l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
@@ -255,7 +352,7 @@ def run_ours(args, ws, rank, local, pg):
     total_pairs = sum_over_ranks(pairs_step, pg)
     value = total_pairs / t_step
 
-    # the all-FP32 form: the same batch with every pair term in FP32 (ER_PREC_COMP)
+    # the all-FP32 form: every pair term in FP32 (ER_PREC_COMP)
     comp = ctx.batch_plan(jobs, er.ER_BATCH_PERSISTENT | er.ER_BATCH_AUTOTUNE |
                           er.ER_BATCH_COMP)
     ctimes = time_plan(ctx, comp, max(2, args.steps // 2), 1, l2buf)
@@ -269,6 +366,8 @@ def run_ours(args, ws, rank, local, pg):
     plain_value = total_pairs / t_plain
     plain_launches = plain.launches
     plain.close()
+    plan.run()  # outs hold the default-mode grids for the error check below
+    ctx.synchronize()
 
     # e2e through the C ABI with host buffers
     ref_outs = [o.cpu().numpy().copy() for o in outs[:2]]
@@ -309,13 +408,14 @@ def run_ours(args, ws, rank, local, pg):
     t_e2e = max_over_ranks(sum(e2e_times) / len(e2e_times), pg)
 
     # roofline of the dominant (persistent) kernel
-    achieved = pairs_step * PAIR_INSTR / (sum(times) / len(times))
+    t_kernel = sum(times) / len(times)
+    achieved = pairs_step * PAIR_INSTR / t_kernel
     roof = {"bound": "fp32", "achieved": achieved / 1e12, "peak": fp32_rate / 1e12,
             "unit": "Tinst/s", "frac": achieved / fp32_rate,
             "peak_source": "measured FP32 FFMA issue rate (er_probe_fp32_rate) on this GPU",
             "traffic": load_traffic(points_step)}
     # the grid store against the measured HBM copy bandwidth (not the bound)
-    roof["grid_store_gbs"] = 4.0 * points_step / (sum(times) / len(times)) / 1e9
+    roof["grid_store_gbs"] = 4.0 * points_step / t_kernel / 1e9
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         hbm = json.load(open(peaks_path)).get("hbm_gbs")
@@ -327,8 +427,8 @@ def run_ours(args, ws, rank, local, pg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic (seeded frameworks; no dataset ships with the reference)",
-        "config": {"workload": f"{len(fws)}-framework batched LJ grids (config 2)",
-                   "frameworks": len(fws),
+        "config": {"workload": WORKLOAD,
+                   "frameworks": len(fws), "precision": "ER_PREC_NEAR64 (default)",
                    "grid_points_per_step": int(points_step), "pair_terms_per_step": int(pairs_step),
                    "cutoff_A": 12.5, "spacing_A": [0.1, 0.2],
                    "l2": "flushed between timed steps (256 MB write)",
@@ -343,37 +443,66 @@ def run_ours(args, ws, rank, local, pg):
         "plain": {"value": plain_value, "unit": "pair-terms/s", "launches_per_step": plain_launches,
                   "batched_over_plain": value / plain_value},
         "comp": {"value": total_pairs / t_comp, "unit": "pair-terms/s",
-                 "ms_per_step": t_comp * 1e3,
+                 "ms_per_step": t_comp * 1e3, "roofline_frac":
+                     pairs_step * PAIR_INSTR / (sum(ctimes) / len(ctimes)) / fp32_rate,
                  "note": "same batch with every pair term in FP32 (ER_PREC_COMP): faster, "
                          "but outside 1e-5 relative on some E < 0 points"},
     }
+    cores = os.cpu_count() or 1
+    if rank == 0 and ws == 1 and not args.no_errors:
+        line["errors"] = {"grids": grid_errors_block(fws, outs, cores)}
+    del outs
     # the Widom and serving forms of the metric, at N = 1 (the batch above is
     # the scaled workload)
     if ws == 1:
         line["config1"] = run_config1(ctx)
         line["extras"] = run_extras(ctx)
+        line["batch_small"] = run_batch_small(ctx, fws, l2buf, fp32_rate)
     if ws == 1 and not args.no_widom:
-        line["widom"] = run_widom(ctx, args)
+        line["widom"] = run_widom(ctx, args, fp32_rate, errors=not args.no_errors)
+        if "kh_errors" in line["widom"]:
+            line.setdefault("errors", {})["kh"] = line["widom"].pop("kh_errors")
     if ws == 1 and not args.no_serving:
         line["serving"] = run_serving(ctx, args)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        starts = np.cumsum([0] + [int(np.prod(f.dims)) for f in fws])
-
-        def sheet_pairs(k, i):
-            f = fws[k]
-            u = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
-            c = ctx.count_pairs(u, f.dims)
-            u.release()
-            return float(c[i].astype(np.float64).sum())
-
-        line["cpu_baseline"] = cpu_baseline(fws, sheet_pairs)
+        from emptyroom_b200 import synth
+        line["cpu_baseline"] = cpu_baseline(fws, synth.config4(1)[0])
         line["cpu_baseline"]["config1_grid_s"] = cpu_config1_grid()
         line["cpu_baseline"]["pockets_129cube_s"] = cpu_pockets_ref()
     ctx.close()
     return line
 
 
-def run_widom(ctx, args):
+def run_batch_small(ctx, fws, l2buf, fp32_rate, dims=(32, 32, 32)):
+    """Many small jobs, where one launch per job leaves the GPU idle: the 256
+    batch frameworks each on a 32^3 grid (the config-1 grid size: 16-32
+    bricks per job against 444 resident CTA slots), one persistent launch
+    against one plain launch per job (both graph-replayed, default mode)."""
+    import torch
+
+    import emptyroom_b200 as er
+    ups = upload_all(ctx, fws)
+    pairs = float(sum(count_pairs(ctx, ups, [dims] * len(fws))))
+    outs = [torch.empty(dims, dtype=torch.float32, device="cuda") for _ in fws]
+    jobs = [(u, dims, o.data_ptr()) for u, o in zip(ups, outs)]
+    res = {"workload": f"{len(fws)} batch frameworks, each on a {dims[0]}^3 grid",
+           "pair_terms_per_step": int(pairs)}
+    for name, mode in (("persistent", er.ER_BATCH_PERSISTENT), ("plain", er.ER_BATCH_PLAIN)):
+        plan = ctx.batch_plan(jobs, mode | er.ER_BATCH_AUTOTUNE)
+        ts = time_plan(ctx, plan, 10, 3, l2buf)
+        t = sum(ts) / len(ts)
+        res[name] = {"ms_per_step": t * 1e3, "pair_terms_per_s": pairs / t,
+                     "launches_per_step": plan.launches,
+                     "roofline_frac": pairs * PAIR_INSTR / t / fp32_rate}
+        plan.close()
+    res["persistent_over_plain"] = res["persistent"]["pair_terms_per_s"] / \
+        res["plain"]["pair_terms_per_s"]
+    for u in ups:
+        u.release()
+    return res
+
+
+def run_widom(ctx, args, fp32_rate, errors=True):
     """Widom batch (config 4): per framework the 0.2 A grid, its pocket mask by
     GPU connected-components labelling, then er_henry with that device mask;
     64 frameworks x 1e7 insertions, Xe at 298 K. Timed through er_henry_batch
@@ -404,7 +533,6 @@ def run_widom(ctx, args):
     # the sequence of single calls (one stream, host round trips in between)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
     e0.record(s)
     seq = [one(k, u) for k, u in enumerate(ups)]
     e1.record(s)
@@ -416,34 +544,117 @@ def run_widom(ctx, args):
     t0 = time.perf_counter()
     kh, npk = ctx.henry_batch(ups, T, n_ins, seeds, block_dims=dims)
     dev = time.perf_counter() - t0
-    wall = dev
     res = list(zip(npk, kh))
     assert [r[1] for r in res] == [r[1] for r in seq]  # bit for bit
     # pair terms: exact for the grids; for the insertions the grid's mean
     # in-cutoff pairs per point (insertions are uniform in the cell)
     grid_pairs = ins_pairs = 0.0
+    mean_pairs = []
     for u in ups:
         ctx.count_pairs_device(u, dims, cnt.data_ptr())
         ctx.synchronize()
         c = float(cnt.double().sum().item())
         grid_pairs += c
-        ins_pairs += c / float(np.prod(dims)) * n_ins
+        mean_pairs.append(c / float(np.prod(dims)))
+        ins_pairs += mean_pairs[-1] * n_ins
+    # the Widom pipeline of one framework alone (Philox points, bin sort,
+    # energy kernel, FP64 log-sum-exp), device-timed on the library's stream:
+    # the denominator of its roofline is the whole pipeline, not the energy
+    # kernel alone, so the fraction is a lower bound for that kernel
+    ctx.grid_device(ups[0], dims, g.data_ptr())
+    ctx.block_pockets_device(g.data_ptr(), dims, T, m.data_ptr())
+    ts = []
+    for k in range(4):
+        e0.record(s)
+        ctx.henry_device_mask(ups[0], T, n_ins, 0, m.data_ptr(), dims)
+        e1.record(s)
+        e1.synchronize()
+        if k:
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+    t_pipe = min(ts)
+    unblocked = n_ins - seq[0][1]["n_blocked"]
+    pipe_pairs = mean_pairs[0] * unblocked
+    total_ins = n_ins * len(fws)
+    out = {"workload": f"{len(fws)} config-1 cells, Xe 298 K: 0.2 A grid {list(dims)} -> "
+                       f"GPU pocket mask -> {n_ins:.0e} Philox insertions each (config 4)",
+           "insertions_per_s": total_ins / dev, "unit": "insertions/s",
+           "ms_per_step": dev * 1e3,
+           "timing": "host clock around er_henry_batch (synchronised before; the call "
+                     "returns when all results are on the host)",
+           "sequential_single_calls": {"ms_per_step": seq_s * 1e3,
+                                       "insertions_per_s": total_ins / seq_s},
+           "pair_terms_per_s": (grid_pairs + ins_pairs) / dev,
+           "pair_terms_note": "grid pairs exact; insertion pairs = insertions x grid mean",
+           "n_pockets_total": int(sum(r[0] for r in res)),
+           "n_blocked_total": int(sum(r[1]["n_blocked"] for r in res)),
+           "roofline": {"bound": "fp32", "unit": "Tinst/s", "peak": fp32_rate / 1e12,
+                        "achieved": pipe_pairs * PAIR_INSTR / t_pipe / 1e12,
+                        "frac": pipe_pairs * PAIR_INSTR / t_pipe / fp32_rate,
+                        "pipeline_ms_per_1e7": t_pipe * 1e3 * 1e7 / n_ins,
+                        "note": "one framework's whole Widom pipeline on the library's "
+                                "stream (CUDA events): a lower bound for the energy kernel"}}
+    if errors:
+        out["kh_errors"] = kh_errors(ctx, fws, ups, res, T, n_ins, dims)
     for u in ups:
         u.release()
-    total_ins = n_ins * len(fws)
-    return {"workload": f"{len(fws)} config-1 cells, Xe 298 K: 0.2 A grid {list(dims)} -> "
-                        f"GPU pocket mask -> {n_ins:.0e} Philox insertions each (config 4)",
-            "insertions_per_s": total_ins / dev, "unit": "insertions/s",
-            "ms_per_step": dev * 1e3, "wall_ms_per_step": wall * 1e3,
-            "timing": "host clock around er_henry_batch (synchronised before; the call "
-                      "returns when all results are on the host)",
-            "sequential_single_calls": {"ms_per_step": seq_s * 1e3,
-                                        "insertions_per_s": total_ins / seq_s},
-            "pair_terms_per_s": (grid_pairs + ins_pairs) / dev,
-            "pair_terms_note": "grid pairs exact; insertion pairs = insertions x grid mean",
-            "n_pockets_total": int(sum(r[0] for r in res)),
-            "n_blocked_total": int(sum(r[1]["n_blocked"] for r in res)),
-            "kh_mol_m3_pa_first": res[0][1]["kh_mol_m3_pa"]}
+    return out
+
+
+def kh_errors(ctx, fws, ups, res, T, n_ins, dims, picks=(0, 21, 42, 63)):
+    """K_H of four config-4 frameworks at the full insertion count, from the
+    timed er_henry_batch, against the FP64 oracle: the oracle's own 0.2 A grid
+    and pocket blocking (the reference's flood fill restated), the same Philox
+    points, the cell-list sum of the reference's terms."""
+    import torch
+
+    import oracle
+    cores = os.cpu_count() or 1
+    out = {"workload": f"config-4 frameworks {list(picks)}, {n_ins:.0e} insertions each, "
+                       "Xe 298 K, pockets masked"}
+    rows = []
+    g = torch.empty(dims, dtype=torch.float32, device="cuda")
+    m = torch.empty(dims, dtype=torch.uint8, device="cuda")
+    for k in picks:
+        if k >= len(fws):
+            continue
+        f = fws[k]
+        P = f.particles()
+        ctx.grid_device(ups[k], dims, g.data_ptr())
+        ctx.block_pockets_device(g.data_ptr(), dims, T, m.data_ptr())
+        ctx.synchronize()
+        mask_gpu = m.cpu().numpy()
+        t0 = time.perf_counter()
+        E = oracle.grid_cells(P, f.t_matrix, f.rep, f.rc2, dims, n_threads=cores)
+        blocked, n_p, _ = oracle.block_pockets(E, T)
+        mask_o = ((blocked == 1e13) & (E != 1e13)).astype(np.uint8)
+        o = oracle.henry_cells(P, f.t_matrix, f.rep, f.rc2, T, k, n_ins, mask=mask_o,
+                               n_threads=cores)
+        kh_o = o["sum_w"] / n_ins / T / 8.314
+        kh = res[k][1]["kh_mol_m3_pa"]
+        rows.append({"fw": k, "kh_rel_err": abs(kh - kh_o) / kh_o, "kh_gpu": kh,
+                     "kh_oracle": kh_o, "mask_equal": bool(np.array_equal(mask_gpu, mask_o)),
+                     "n_pockets": [res[k][0], n_p],
+                     "n_blocked": [int(res[k][1]["n_blocked"]), int(o["n_blocked"])],
+                     "oracle_s": time.perf_counter() - t0})
+    out["per_framework"] = rows
+    out["max_rel_err"] = max(r["kh_rel_err"] for r in rows) if rows else None
+    return out
+
+
+def cpu_config1_grid():
+    """The reference's ComputeGridSheet on the whole config-1 32^3 grid, all
+    host cores (seconds)."""
+    import oracle
+    from emptyroom_b200 import synth
+    f = synth.config1(0)
+    P = f.particles()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    if oracle.ref_available():
+        oracle.ref_grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
+    else:
+        oracle.grid(P, f.t_matrix, f.rep, f.rc2, (32, 32, 32), n_threads=cores)
+    return time.perf_counter() - t0
 
 
 def run_config1(ctx):
@@ -608,82 +819,164 @@ def load_traffic(points_step):
 
 
 def run_reference(args, ws, rank):
-    """The reference's own CPU implementation (ComputeGridSheet compiled from
-    its sources, oracle/_ref) on a bounded sample of the same workload."""
+    """The reference's own CPU implementation on the host cores: its
+    ComputeGridSheet (oracle/_ref, compiled from its sources) on a bounded
+    sample of the batch's grids each step, and its LJ routine at Widom
+    insertion points. The frameworks come from oracle/workloads.py (this
+    library is not loaded)."""
     import oracle
+    from oracle import workloads
     if rank != 0:
         return None
-    fws = make_workload(0)
+    fws = workloads.config2(256)
     cores = os.cpu_count() or 1
     rng = np.random.default_rng(11)
     step_target = 3.0
-    values = []
+    values, step_s = [], []
     samples = []
-    use_ref = oracle.ref_available()
     for step in range(args.warmup + args.steps):
-        pairs = 0.0
-        t = 0.0
-        while t < step_target:
-            k = int(rng.integers(0, len(fws)))
-            f = fws[k]
-            P = f.particles()
-            i = int(rng.integers(0, f.dims[0]))
-            t0 = time.perf_counter()
-            if use_ref:
-                oracle.ref_grid_sheets(P, f.t_matrix, f.rep, f.rc2, f.dims, [i], n_threads=cores)
-            else:
-                ny, nz = f.dims[1], f.dims[2]
-                jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
-                pts = np.stack([np.full(jj.size, i / (f.dims[0] - 1)), jj.ravel() / (ny - 1),
-                                kk.ravel() / (nz - 1)], -1)
-                oracle.points(P, f.t_matrix, f.rep, f.rc2, pts, n_threads=cores)
-            t += time.perf_counter() - t0
-            ny, nz = f.dims[1], f.dims[2]
-            jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
-            pts = np.stack([np.full(jj.size, i / (f.dims[0] - 1)), jj.ravel() / (ny - 1),
-                            kk.ravel() / (nz - 1)], -1)
-            pairs += oracle.points_pairs(P, f.t_matrix, f.rep, f.rc2, pts,
-                                         n_threads=cores).sum()
-            if step == 0:
-                samples.append(f"fw{k}:x{i}")
+        pairs, secs, sample = ref_grid_sample(fws, step_target, rng, cores)
+        if step == 0:
+            samples = sample
         if step >= args.warmup:
-            values.append(pairs / t)
+            values.append(pairs / secs)
+            step_s.append(secs)
+    n_ins, wpairs, wsecs = ref_widom_sample(workloads.config4(1)[0], 6.0, cores)
     v = float(np.mean(values))
-    kind = "reference" if use_ref else "port"
+    kind = "reference" if oracle.ref_available() else "port"
     return {"metric": METRIC, "value": v, "unit": "pair-terms/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_target * 1e3,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(np.mean(step_s)) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded frameworks)", "impl": "reference",
-            "config": {"workload": "256-framework batched LJ grids (config 2)",
-                       "sample": "whole x-sheets of randomly chosen frameworks, ~3 s per step"},
+            "config": {"workload": WORKLOAD,
+                       "sample": "each step: random grid points of randomly chosen "
+                                 f"frameworks of the batch, ~{step_target:.0f} s of the "
+                                 "reference's ComputeGridSheet on all host cores"},
             "cpu_baseline": {"value": v, "unit": "pair-terms/s", "cores": cores, "kind": kind,
-                             "sample": f"x-sheets {samples[:8]}..., ~{step_target:.0f} s per step"},
+                             "sample": f"256-point chunks of frameworks {samples[:6]}..., "
+                                       f"~{step_target:.0f} s per step"},
+            "widom": {"insertions_per_s": n_ins / wsecs, "pair_terms_per_s": wpairs / wsecs,
+                      "sample": f"first {n_ins} Philox insertions of a config-4 cell (Xe), "
+                                "the reference's LJ routine at each point"},
             "e2e": {"value": v, "unit": "pair-terms/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
 
+def case_precision(ctx, args):
+    """Precision sweep on the config-3 cell (30.1, 32.4, 28.7 A; 85/95/110 deg;
+    CH4; cutoff 12.5 A) on a dims^3 grid, 4096 atoms as specified or
+    --atoms (646 gives the config-1 number density): the ER_PREC_FP32,
+    ER_PREC_COMP and default (NEAR64) grids against the ER_PREC_FP64 grid,
+    itself pinned to the oracle on sampled points."""
+    import emptyroom_b200 as er
+    import oracle
+    from emptyroom_b200 import synth
+    f = synth.config3() if args.atoms == 4096 else synth.make_framework(
+        3, (30.1, 32.4, 28.7), (85.0, 95.0, 110.0), args.atoms, n_types=4, probe="CH4",
+        rc=12.5, d_min=1.2, name=f"config3_{args.atoms}")
+    P = f.particles()
+    fw = ctx.upload(P, f.t_matrix, f.rep, f.rc2)
+    dims = (args.dims,) * 3
+    e64 = ctx.grid(fw, dims, precision=er.ER_PREC_FP64, f64=True)
+    rng = np.random.default_rng(7)
+    idx = rng.integers(0, args.dims, size=(4000, 3))
+    pts = idx / (args.dims - 1.0)
+    ref, S, _ = oracle.points_cells(P, f.t_matrix, f.rep, f.rc2, pts, 1e-12)
+    got = e64[idx[:, 0], idx[:, 1], idx[:, 2]]
+    ok = ref < er.ER_ENERGY_CAP
+    res = {"workload": f"config-3 cell, {args.atoms} atoms, {args.dims}^3 grid, CH4, rc 12.5 A",
+           "fp64_grid_vs_oracle_max_over_sum_abs": float(
+               np.max(np.abs(got[ok] - ref[ok]) / np.maximum(S[ok], 1e-300))),
+           "modes": {}}
+
+    def stats(e):
+        e = e.astype(np.float64)
+        out = {"cap_agrees": bool(np.array_equal(e >= er.ER_ENERGY_CAP, e64 >= er.ER_ENERGY_CAP))}
+        for name, msk in (("neg", e64 < 0), ("below_-1K", e64 < -1.0),
+                          ("below_-10K", e64 < DEEP), ("pos", (e64 >= 0) & (e64 < 1e10))):
+            d = np.abs(e[msk] - e64[msk])
+            r = d / np.maximum(np.abs(e64[msk]), 1e-30)
+            out[name] = {"n": int(msk.sum()),
+                         "abs_max": float(d.max()) if d.size else 0.0,
+                         "abs_p99": float(np.percentile(d, 99)) if d.size else 0.0,
+                         "rel_max": float(r.max()) if r.size else 0.0,
+                         "rel_p99": float(np.percentile(r, 99)) if r.size else 0.0,
+                         "frac_rel_le_1e-5": float(np.mean(r <= 1e-5)) if r.size else 1.0}
+        return out
+
+    for name, flags in (("fp32", er.ER_PREC_FP32), ("comp", er.ER_PREC_COMP),
+                        ("near64_default", er.ER_PREC_NEAR64)):
+        res["modes"][name] = stats(ctx.grid(fw, dims, precision=flags))
+    fw.release()
+    print(json.dumps(res, indent=1))
+
+
+def case_refgpu(ctx, args):
+    """The reference's own GPU writegrid (oracle/_ref/writegrid, its sources
+    compiled for sm_100a) beside this library on the same B200 and case: the
+    config-1 cell at 0.2 A (129^3 points). Writes the project tree the
+    reference reads into --tree and prints this library's grid time (CUDA
+    events, er_grid into device memory) and the exact pair count; the
+    reference's kernel times come from an ncu launch list of its writegrid
+    run in that tree."""
+    import torch
+
+    from emptyroom_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fixture_tree import write_tree
+    f = synth.config1(0)
+    name, ads = write_tree(args.tree, f, resolution=0.2)
+    dims = synth.grid_dims_for(f.abc, 0.2)
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    out = torch.empty(dims, dtype=torch.float32, device="cuda")
+    s = torch.cuda.ExternalStream(ctx.stream_ptr)
+    ts = []
+    for k in range(6):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.grid_device(fw, dims, out.data_ptr())
+        e1.record(s)
+        e1.synchronize()
+        if k >= 2:
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+    ctx.count_pairs_device(fw, dims, out.data_ptr())
+    ctx.synchronize()
+    pairs = float(out.double().sum().item())
+    t = min(ts)
+    print(json.dumps({"framework": name, "adsorbate": ads, "dims": list(dims), "pairs": pairs,
+                      "ours_s": t, "ours_pair_terms_per_s": pairs / t}))
+
+
 def run_case(args):
-    """Single-kernel cases for profiling: `config3` runs the 4096-atom triclinic
+    """Single-kernel and analysis cases: `config3` runs the 4096-atom triclinic
     cell on a dims^3 grid (one er_grid launch per step); `widom` runs er_henry
-    with --insertions points on a config-1 cell."""
+    with --insertions points on a config-1 cell; `precision` the precision
+    sweep; `refgpu` this library beside the reference's own GPU writegrid."""
     import torch
 
     import emptyroom_b200 as er
     from emptyroom_b200 import synth
     ctx = er.Context(0)
-    if args.case == "config3":
+    if args.case == "precision":
+        case_precision(ctx, args)
+    elif args.case == "refgpu":
+        case_refgpu(ctx, args)
+    elif args.case == "config3":
         f = synth.config3()
         fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
         dims = (args.dims,) * 3
         out = torch.empty(dims, dtype=torch.float32, device="cuda")
         s = torch.cuda.ExternalStream(ctx.stream_ptr)
-        tile = er.ER_TILE_P8 if args.tile == 8 else 0
+        flags = (er.ER_TILE_P8 if args.tile == 8 else 0) | \
+            (er.ER_PREC_COMP if args.precision == "comp" else 0)
         times = []
         for k in range(args.warmup + args.steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(s)
-            ctx.grid_device(fw, dims, out.data_ptr(), precision=tile)
+            ctx.grid_device(fw, dims, out.data_ptr(), precision=flags)
             e1.record(s)
             e1.synchronize()
             if k >= args.warmup:
@@ -693,8 +986,8 @@ def run_case(args):
         ctx.synchronize()
         pairs = float(cnt.double().sum().item())
         t = sum(times) / len(times)
-        print(json.dumps({"case": "config3", "dims": dims, "tile_p": args.tile, "ms": t * 1e3,
-                          "pairs": pairs,
+        print(json.dumps({"case": "config3", "dims": dims, "tile_p": args.tile,
+                          "precision": args.precision, "ms": t * 1e3, "pairs": pairs,
                           "pair_terms_per_s": pairs / t,
                           "pairs_per_point": pairs / float(np.prod(dims))}))
     else:
@@ -719,10 +1012,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="batch", choices=["batch", "config3", "widom"])
+    ap.add_argument("--no-errors", action="store_true",
+                    help="skip the oracle comparison of the grids and K_H")
+    ap.add_argument("--case", default="batch",
+                    choices=["batch", "config3", "widom", "precision", "refgpu"])
     ap.add_argument("--dims", type=int, default=256)
+    ap.add_argument("--atoms", type=int, default=4096)
+    ap.add_argument("--tree", default="/tmp/er_tree")
     ap.add_argument("--insertions", type=int, default=10_000_000)
     ap.add_argument("--tile", type=int, default=4, choices=[4, 8])
+    ap.add_argument("--precision", default="near64", choices=["near64", "comp"])
     ap.add_argument("--frameworks", type=int, default=256,
                     help="frameworks of the batch (256 is the workload; fewer for profiling)")
     ap.add_argument("--no-widom", action="store_true")

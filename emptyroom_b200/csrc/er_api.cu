@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "er_ctx.h"
+#include "er_nvtx.h"
 #include "er_engine.cuh"
 #include "er_host.h"
 
@@ -570,11 +571,13 @@ void fw_record(const HostFramework& hf, size_t n_img, const FwLayout& L, void* b
 extern "C" {
 
 int er_framework_upload(er_ctx* ctx, const er_framework_desc* desc, int* fw_id) {
+    er::NvtxRange nvtx("er_framework_upload");
     if (!ctx || !desc || !fw_id) return ER_ERR_INVALID;
     return host_upload_many(ctx, desc, 1, fw_id);
 }
 
 int er_framework_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw_ids) {
+    er::NvtxRange nvtx("er_framework_upload_many");
     if (!ctx || n < 0 || (n > 0 && (!descs || !fw_ids))) return ER_ERR_INVALID;
     if (n == 0) return ER_OK;
     return device_upload_many(ctx, descs, n, fw_ids);
@@ -669,6 +672,7 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes) {
 }
 
 int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out) {
+    er::NvtxRange nvtx("er_grid");
     if (!ctx || !out) return ER_ERR_INVALID;
     if (int st = check_grid_dims(ctx, nx, ny, nz, "grid")) return st;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -947,6 +951,7 @@ int er_batch_plan_create(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int m
 }
 
 int er_batch_plan_run(er_batch_plan* p) {
+    er::NvtxRange nvtx("er_batch_plan_run");
     if (p && !p->exec) return ER_ERR_INVALID;
     if (!p) return ER_ERR_INVALID;
     ER_CUDA(p->ctx, cudaGraphLaunch(p->exec, p->ctx->stream));
@@ -975,6 +980,7 @@ void er_batch_plan_destroy(er_batch_plan* p) {
 }
 
 int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
+    er::NvtxRange nvtx("er_grid_batch");
     if (!ctx || n_jobs < 0 || (n_jobs > 0 && !jobs)) return ER_ERR_INVALID;
     if (mode & ER_BATCH_HOST_OUT) {
         // stage every grid in one device buffer; copy each back as soon as

@@ -780,13 +780,10 @@ static __device__ __noinline__ void recheck_borderline(EngineSmem& s, const Pol&
     }
 }
 
-// Kept out of line: the producer's loop state (box, cell ranges, counters)
-// is saved once around the call instead of staying live in registers
-// through the pair loops.
 template <class Pol, int PREC>
-static __device__ __noinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
-                                               const CutoffConsts& cc, int n_cand,
-                                               Lane<Pol, PREC>& L) {
+__device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, const FwDev& fw,
+                                                const CutoffConsts& cc, int n_cand,
+                                                Lane<Pol, PREC>& L) {
     constexpr int P = Pol::kP;
     constexpr bool kNear = PrecTraits<PREC>::near64;
     constexpr bool kF64 = PrecTraits<PREC>::fp64;
@@ -991,6 +988,29 @@ static __device__ __noinline__ void warp_flush(EngineSmem& s, const Pol& pol, co
             for (int p = 0; p < kNearP; ++p) tot_at(s, p0 + p) += nacc[p];
         }
     }
+}
+
+// Lattice (grid) flushes run out of line: the producer's loop state (box,
+// cell ranges, counters) is saved once around the call instead of staying
+// live in registers through the pair loops (at the 80-register limit of three
+// CTAs per SM that took the 256-framework batch from 370 to 357 ms). The
+// Widom kernel (128 registers, generic points) is faster with the flush
+// inlined (1.89 against 2.18 ms per 1e7 insertions).
+template <class Pol, int PREC>
+static __device__ __noinline__ void warp_flush_call(EngineSmem& s, const Pol& pol,
+                                                    const FwDev& fw, const CutoffConsts& cc,
+                                                    int n_cand, Lane<Pol, PREC>& L) {
+    warp_flush_body<Pol, PREC>(s, pol, fw, cc, n_cand, L);
+}
+
+template <class Pol, int PREC>
+__device__ __forceinline__ void warp_flush(EngineSmem& s, const Pol& pol, const FwDev& fw,
+                                           const CutoffConsts& cc, int n_cand,
+                                           Lane<Pol, PREC>& L) {
+    if constexpr (Pol::kLattice)
+        warp_flush_call<Pol, PREC>(s, pol, fw, cc, n_cand, L);
+    else
+        warp_flush_body<Pol, PREC>(s, pol, fw, cc, n_cand, L);
 }
 
 template <class Pol, int PREC>

@@ -15,6 +15,7 @@
 #include <algorithm>
 
 #include "er_ctx.h"
+#include "er_nvtx.h"
 #include "er_engine.cuh"
 #include "er_philox.h"
 
@@ -32,12 +33,22 @@ struct Lse {
     double m, s, se;
 };
 
+// Bin of a point: bins grouped in 2x2x2 bricks, bricks in serpentine order
+// (y runs backwards on odd x layers, z backwards on the odd rows of the
+// traversal), so consecutive bricks are always face neighbours and any run of
+// consecutive sorted points -- a warp's or a CTA's -- spans a compact box, also
+// where it straddles the end of a brick row (plain row order would put the
+// next brick at the far side of the cell there).
 __device__ __forceinline__ int bin_key(const double* f, const BinGeom& g) {
     int b[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) b[d] = min(g.nb[d] - 1, max(0, (int)(f[d] * g.nb[d])));
-    return (((b[0] >> 1) * g.NB[1] + (b[1] >> 1)) * g.NB[2] + (b[2] >> 1)) * 8 +
-           ((b[0] & 1) << 2) + ((b[1] & 1) << 1) + (b[2] & 1);
+    const int bx = b[0] >> 1;
+    int by = b[1] >> 1, bz = b[2] >> 1;
+    if (bx & 1) by = g.NB[1] - 1 - by;
+    if ((bx * g.NB[1] + by) & 1) bz = g.NB[2] - 1 - bz;
+    return ((bx * g.NB[1] + by) * g.NB[2] + bz) * 8 + ((b[0] & 1) << 2) + ((b[1] & 1) << 1) +
+           (b[2] & 1);
 }
 
 // Corner test of the pocket mask; the cell lookup follows src/gcmc.cc:155-157.
@@ -451,6 +462,7 @@ using namespace er;
 extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t seed,
                         const uint8_t* block_mask, int mnx, int mny, int mnz,
                         er_henry_result* out, float* energies_out) {
+    er::NvtxRange nvtx("er_henry");
     if (!ctx || !out) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     const FwRecord* f = find_fw(ctx, fw_id);
@@ -517,6 +529,7 @@ extern "C" int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temp
                               int64_t n_insertions, const uint64_t* seeds, int block_nx,
                               int block_ny, int block_nz, er_henry_result* results,
                               int* n_pockets) {
+    er::NvtxRange nvtx("er_henry_batch");
     if (!ctx || n < 0 || (n > 0 && (!fw_ids || !seeds || !results))) return ER_ERR_INVALID;
     if (n == 0) return ER_OK;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "er_ctx.h"
+#include "er_nvtx.h"
 
 namespace er {
 
@@ -429,6 +430,7 @@ using namespace er;
 
 extern "C" int er_block_pockets(er_ctx* ctx, double* grid, int nx, int ny, int nz,
                                 double temperature, int* n_pockets, int* segments_out) {
+    er::NvtxRange nvtx("er_block_pockets");
     if (!ctx || !grid || !n_pockets) return ER_ERR_INVALID;
     int stt = check_dims(ctx, nx, ny, nz, temperature);
     if (stt != ER_OK) return stt;
@@ -486,6 +488,7 @@ int block_pockets_device_on(er_ctx* ctx, PocketScratch& ps, cudaStream_t st, con
 extern "C" int er_block_pockets_device(er_ctx* ctx, const float* grid, int nx, int ny, int nz,
                                        double temperature, uint8_t* pocket_mask_out,
                                        int* n_pockets) {
+    er::NvtxRange nvtx("er_block_pockets_device");
     if (!ctx || !grid || !pocket_mask_out || !n_pockets) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     return block_pockets_device_on(ctx, ctx->pocket, ctx->stream, grid, nx, ny, nz, temperature,

@@ -38,6 +38,7 @@
 
 #include "er_ctx.h"
 #include "er_engine.cuh"
+#include "er_nvtx.h"
 
 namespace {
 
@@ -305,6 +306,8 @@ struct er_server {
         f->second.last_use = tick;
         f->second.pins++;
         j.st.start_s = now();
+        er::NvtxRange nvtx(job.kind == ER_JOB_GRID ? "server grid job launch"
+                                                   : "server Henry job launch");
         int st = ER_OK;
         if (job.kind == ER_JOB_GRID) {
             SrvGrid g;

@@ -334,8 +334,12 @@ int er_server_submit(er_server* s, const er_job* job, uint64_t* ticket);
 int er_server_poll(er_server* s, uint64_t ticket, er_job_status* st);
 /* Waits up to timeout_s for the job; ER_ERR_TIMEOUT when it is still running. */
 int er_server_wait(er_server* s, uint64_t ticket, double timeout_s, er_job_status* st);
-/* Device pointer of a finished grid job's resident grid (valid until that
- * grid is evicted or the server is destroyed). */
+/* Device pointer of a finished grid job's resident grid, valid until that
+ * grid is evicted or the server is destroyed. Once the budget is full, an
+ * evicted grid's buffer may be taken over by a later grid job and hold
+ * another framework's grid: a caller that keeps using the pointer must not
+ * submit grid jobs in the meantime, and orders its own reads (on its own
+ * streams) itself, since only server jobs pin a grid. */
 int er_server_grid(er_server* s, uint64_t ticket, const float** grid);
 /* Server clock (seconds), the clock of er_job_status. */
 double er_server_now(const er_server* s);

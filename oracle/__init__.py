@@ -62,6 +62,9 @@ def lib():
                                            ctypes.c_int, _u8p, ctypes.c_int]
         L.oracle_philox4x32_10.restype = None
         L.oracle_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+        L.oracle_insertion_points.restype = None
+        L.oracle_insertion_points.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64,
+                                              _dp]
         L.oracle_insertion_point.restype = None
         L.oracle_insertion_point.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _dp]
         L.oracle_henry.restype = None
@@ -118,6 +121,9 @@ def ref():
         R.ref_grid_sheets.argtypes = [_dp, ctypes.c_int, _dp, _ip, ctypes.c_double,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int,
                                       _dp, ctypes.c_int]
+        R.ref_points.restype = None
+        R.ref_points.argtypes = [_dp, ctypes.c_int, _dp, _ip, ctypes.c_double, _dp,
+                                 ctypes.c_int64, _dp, ctypes.c_int]
         R.ref_accessibility.restype = None
         R.ref_accessibility.argtypes = [_dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, _dp, ctypes.c_int]
@@ -218,6 +224,13 @@ def philox4x32_10(ctr, key):
 def insertion_point(seed, i):
     o = np.empty(3, dtype=np.float64)
     lib().oracle_insertion_point(int(seed), int(i), _ptr(o, _dp))
+    return o
+
+
+def insertion_points(seed, n, i0=0):
+    """Insertion points i0 .. i0 + n - 1 of Philox stream `seed` (n x 3)."""
+    o = np.empty((int(n), 3), dtype=np.float64)
+    lib().oracle_insertion_points(int(seed), int(i0), int(n), _ptr(o, _dp))
     return o
 
 
@@ -364,6 +377,19 @@ def ref_grid_sheets(particles, t, rep, rc2, dims, sheets, n_threads=0):
     R.ref_grid_sheets(_ptr(p, _dp), len(p), _ptr(tm, _dp), _ptr(r, _ip), float(rc2), nx, ny,
                       nz, _ptr(sh, _ip), len(sh), _ptr(out, _dp), int(n_threads))
     return out.reshape(len(sh), ny, nz)
+
+
+def ref_points(particles, t, rep, rc2, pts, n_threads=0):
+    """The reference's ComputeGridSheet at arbitrary fractional points (n x 3)."""
+    R = ref()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libref.so not built")
+    p, tm, r = _prep(particles, t, rep)
+    q = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    out = np.empty(len(q), dtype=np.float64)
+    R.ref_points(_ptr(p, _dp), len(p), _ptr(tm, _dp), _ptr(r, _ip), float(rc2), _ptr(q, _dp),
+                 len(q), _ptr(out, _dp), int(n_threads))
+    return out
 
 
 def ref_accessibility(particles, t, dims, n_threads=0):

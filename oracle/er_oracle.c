@@ -339,6 +339,10 @@ void oracle_insertion_point(uint64_t seed, uint64_t i, double out[3]) {
     out[2] = u53(s[0], s[1]);
 }
 
+void oracle_insertion_points(uint64_t seed, uint64_t i0, int64_t n, double* out) {
+    for (int64_t k = 0; k < n; k++) oracle_insertion_point(seed, i0 + (uint64_t)k, out + 3 * k);
+}
+
 /* An insertion is blocked when any of the 8 corners of its grid cell is set.
  * Cell lookup follows src/gcmc.cc:155-157 (floor(x_f / dx_f), dx_f = 1/(N-1)). */
 int oracle_insertion_blocked(const uint8_t* mask, int nx, int ny, int nz, const double p[3]) {

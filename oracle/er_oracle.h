@@ -80,6 +80,8 @@ void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t
 /* Fractional insertion point i of stream `seed`, each coordinate uniform in
  * [0,1) with 53 random bits. Replaces the MTGP32 darts of src/doHenry.h:53-55. */
 void oracle_insertion_point(uint64_t seed, uint64_t i, double out[3]);
+/* Points i0 .. i0 + n - 1 of stream seed into out (n x 3). */
+void oracle_insertion_points(uint64_t seed, uint64_t i0, int64_t n, double* out);
 
 /* Widom statistics over insertions [0, n_ins) of stream `seed`
  * (src/doHenry.h:53-125 per insertion, src/henry.cu:157-174 reduction).

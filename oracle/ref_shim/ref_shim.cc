@@ -121,9 +121,70 @@ void run_grid(const double* particles, int n_atoms, const double* t, const int* 
     for (int k = 0; k < nth; k++) pthread_join(th[k], nullptr);
 }
 
+struct PointJob {
+    const FrameworkParticle* atoms;
+    const GridParameters* params;
+    const double* pts;
+    int64_t n_pts;
+    double* out;
+    int tid, nth;
+};
+
+// ComputeGridSheet on one-point axes: thread (0, 0) of block (0, 0) computes
+// the point (pts[3i], pts[3i+1], pts[3i+2]) -- the reference's LJ routine at
+// an arbitrary point, e.g. a Widom insertion (src/doHenry.h:70-98 is the same
+// sum with min_r 1e-16 instead of 1e-12).
+void* point_worker(void* arg) {
+    PointJob* jb = static_cast<PointJob*>(arg);
+    GridParameters p = *jb->params;
+    p.N_x = 1; p.N_y = 1; p.N_z = 1;
+    blockDim.x = 16; blockDim.y = 16; blockDim.z = 1;
+    blockIdx.x = blockIdx.y = blockIdx.z = 0;
+    threadIdx.x = threadIdx.y = threadIdx.z = 0;
+    for (int64_t i = jb->tid; i < jb->n_pts; i += jb->nth) {
+        double y = jb->pts[3 * i + 1], z = jb->pts[3 * i + 2], e = 0.0;
+        ComputeGridSheet(&z, &y, &e, const_cast<FrameworkParticle*>(jb->atoms), p,
+                         jb->pts[3 * i]);
+        jb->out[i] = e;
+    }
+    return nullptr;
+}
+
 }  // namespace
 
 extern "C" {
+
+/* The reference's ComputeGridSheet evaluated at n_pts fractional points
+ * (n_pts x 3), threads over points; out[i] = energy at point i. */
+void ref_points(const double* particles, int n_atoms, const double* t, const int* rep,
+                double rc2, const double* pts, int64_t n_pts, double* out, int n_threads) {
+    GridParameters p;
+    p.N_framework_atoms = n_atoms;
+    p.N_x = p.N_y = p.N_z = 1;
+    p.replication_factor_a = rep[0];
+    p.replication_factor_b = rep[1];
+    p.replication_factor_c = rep[2];
+    p.r_cutoff_squared = rc2;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) p.t_matrix[a][b] = t[3 * a + b];
+    std::vector<FrameworkParticle> atoms(n_atoms);
+    for (int a = 0; a < n_atoms; a++) {
+        atoms[a].x_f = particles[5 * a + 0];
+        atoms[a].y_f = particles[5 * a + 1];
+        atoms[a].z_f = particles[5 * a + 2];
+        atoms[a].eps_with_adsorbate = particles[5 * a + 3];
+        atoms[a].sig_with_adsorbate_squared = particles[5 * a + 4];
+    }
+    int nth = n_threads > 0 ? n_threads : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if ((int64_t)nth > n_pts) nth = (int)(n_pts > 0 ? n_pts : 1);
+    std::vector<PointJob> jobs(nth);
+    std::vector<pthread_t> th(nth);
+    for (int k = 0; k < nth; k++) {
+        jobs[k] = PointJob{atoms.data(), &p, pts, n_pts, out, k, nth};
+        pthread_create(&th[k], nullptr, point_worker, &jobs[k]);
+    }
+    for (int k = 0; k < nth; k++) pthread_join(th[k], nullptr);
+}
 
 /* particles: n x 5 doubles in FrameworkParticle order (x_f, y_f, z_f, eps, sig2);
  * t: row-major 3x3; rep: replication factors; out: nx*ny*nz doubles. */
