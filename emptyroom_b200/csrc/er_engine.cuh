@@ -640,7 +640,13 @@ __device__ __forceinline__ int generic_packed_lists(EngineSmem& s, const unsigne
     int q = 0;
     while (q < n_in) {
         const int qe = kComp ? min(q + PrecTraits<PREC>::inner_chunk, n_in) : n_in;
-        for (; q < qe; ++q) inner_atom(wl[q]);
+        // two atoms per iteration: eight independent FP32 chains for the
+        // scheduler (the kernel is latency-bound at two CTAs per SM)
+        for (; q + 1 < qe; q += 2) {
+            inner_atom(wl[q]);
+            inner_atom(wl[q + 1]);
+        }
+        if (q < qe) inner_atom(wl[q++]);
         if (kComp) fold_packed<M>(s, acc2);
     }
     q = 0;
@@ -937,8 +943,20 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
                 nacc[p] = 0.0;
             }
             // atoms inside the cutoff for every point of the warp: no test
+            // Widom points: the next atom's FP64 data is loaded while this one's
+            // terms run (the 128-register Widom kernel has room for it; at the
+            // grid kernels' 80 registers it costs more than it hides)
+            constexpr bool kPrefetch = !Pol::kLattice;
+            Atom64 nxt = (kPrefetch && n_ni > 0) ? atom64(fw, s.cid[wn[0] >> 5], o0, o1, o2)
+                                                 : Atom64{};
             for (int q = 0; q < n_ni; ++q) {
-                const Atom64 a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
+                Atom64 a;
+                if (kPrefetch) {
+                    a = nxt;
+                    if (q + 1 < n_ni) nxt = atom64(fw, s.cid[wn[q + 1] >> 5], o0, o1, o2);
+                } else {
+                    a = atom64(fw, s.cid[wn[q] >> 5], o0, o1, o2);
+                }
                 if (Pol::kLattice) {
                     // a lattice lane's points share y and z: dy^2 + dz^2 once per atom
                     const double dy = qy[0] - a.y, dz = qz[0] - a.z;

@@ -7,10 +7,13 @@
 //   2. scan    bin counts -> bin starts
 //   3. scatter insertion indices into their bins; 4. sort each bin ascending
 //      (so the layout, and with it every FP32 rounding, is deterministic)
-//   5. energy  the shared LJ engine over 2048 sorted points per CTA
+//   5. energy  the shared LJ engine over 2048 (1024 for runs below 1e6)
+//              sorted points per CTA
 //   6. reduce  FP64 log-sum-exp of exp(-E/T) and E exp(-E/T) in insertion
 //              order with a fixed tree: (m, s, se) with sum w = s e^m.
 #include <math.h>
+
+#include <climits>
 
 #include <algorithm>
 
@@ -21,7 +24,14 @@
 
 namespace er {
 
-constexpr int kHenryP = 8;  // insertions per thread of the energy kernel
+// Insertions per thread of the energy kernel: 8 for large runs (1.82 against
+// 2.00 ms per 1e7 insertions on a config-1 cell); 4 below kHenrySmallN, where
+// a run fills few waves of CTAs and more, smaller CTAs finish sooner (0.16
+// against 0.26 ms for 1e5 insertions).
+constexpr int kHenryP = 8;
+constexpr int kHenryPSmall = 4;
+constexpr int64_t kHenrySmallN = 1000000;
+inline int henry_points_per_thread(int64_t n) { return n < kHenrySmallN ? kHenryPSmall : kHenryP; }
 
 struct BinGeom {
     int nb[3];  // bins per fractional axis
@@ -70,10 +80,13 @@ __device__ __forceinline__ bool blocked_at(const uint8_t* mask, int nx, int ny, 
     return false;
 }
 
+// Insertion i: its point, the mask test, its bin key and its slot in the bin
+// (the count before it; slots within a bin are in arbitrary order, which the
+// per-bin sort makes ascending).
 __global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t* __restrict__ mask,
                                  int mnx, int mny, int mnz, int* __restrict__ key,
-                                 int* __restrict__ counts, float* __restrict__ energies,
-                                 int* __restrict__ n_blocked) {
+                                 int* __restrict__ slot, int* __restrict__ counts,
+                                 float* __restrict__ energies, int* __restrict__ n_blocked) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double f[3];
         insertion_point(seed, (uint64_t)i, f);
@@ -84,7 +97,7 @@ __global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t*
         } else {
             const int k = bin_key(f, g);
             key[i] = k;
-            atomicAdd(&counts[k], 1);
+            slot[i] = atomicAdd(&counts[k], 1);
         }
     }
 }
@@ -211,18 +224,19 @@ int scan_exclusive(er_ctx* ctx, const int* in, int n, int* out, int* tile_sums,
     return ER_OK;
 }
 
-__global__ void henry_scatter_kernel(const int* __restrict__ key, int n,
-                                     const int* __restrict__ starts, int* __restrict__ fill,
+__global__ void henry_scatter_kernel(const int* __restrict__ key, const int* __restrict__ slot,
+                                     int n, const int* __restrict__ starts,
                                      int* __restrict__ tmp) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int k = key[i];
-        if (k >= 0) tmp[starts[k] + atomicAdd(&fill[k], 1)] = i;
+        if (k >= 0) tmp[starts[k] + slot[i]] = i;
     }
 }
 
 // One warp per bin: rank of each entry among its bin's entries -> ascending
-// order; the insertion point itself (recomputed from its Philox counter) is
-// written in the same sorted order, so the energy kernel reads it coalesced.
+// order (the bin's entries compared 32 at a time through shuffles); the
+// insertion point itself (recomputed from its Philox counter) is written in the
+// same sorted order, so the energy kernel reads it coalesced.
 __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_keys,
                                        const int* __restrict__ tmp, uint64_t seed,
                                        int* __restrict__ order, double* __restrict__ pts_sorted) {
@@ -230,29 +244,37 @@ __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_key
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n_keys; b += warps) {
         const int s = starts[b], L = starts[b + 1] - s;
-        for (int q = lane; q < L; q += 32) {
-            const int v = tmp[s + q];
+        for (int q0 = 0; q0 < L; q0 += 32) {
+            const int q = q0 + lane;
+            const int v = q < L ? tmp[s + q] : INT_MAX;
             int rank = 0;
-            for (int r = 0; r < L; ++r) rank += tmp[s + r] < v;
-            order[s + rank] = v;
-            double f[3];
-            insertion_point(seed, (uint64_t)v, f);
-            pts_sorted[3 * (size_t)(s + rank)] = f[0];
-            pts_sorted[3 * (size_t)(s + rank) + 1] = f[1];
-            pts_sorted[3 * (size_t)(s + rank) + 2] = f[2];
+            for (int r0 = 0; r0 < L; r0 += 32) {
+                const int u = r0 + lane < L ? tmp[s + r0 + lane] : INT_MAX;
+#pragma unroll
+                for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, u, k) < v;
+            }
+            if (q < L) {
+                order[s + rank] = v;
+                double f[3];
+                insertion_point(seed, (uint64_t)v, f);
+                pts_sorted[3 * (size_t)(s + rank)] = f[0];
+                pts_sorted[3 * (size_t)(s + rank) + 1] = f[1];
+                pts_sorted[3 * (size_t)(s + rank) + 2] = f[2];
+            }
         }
     }
 }
 
+template <int P>
 __global__ void __launch_bounds__(kThreads, 2)
     henry_energy_kernel(const __grid_constant__ PointTask task) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    if ((long long)blockIdx.x * (kWarps * 32 * kHenryP) >= (long long)*task.n_valid) return;
+    if ((long long)blockIdx.x * (kWarps * 32 * P) >= (long long)*task.n_valid) return;
     EngineSmem& s = *reinterpret_cast<EngineSmem*>(smem_raw);
-    PointPolicy<kHenryP> pol(&task, blockIdx.x);
+    PointPolicy<P> pol(&task, blockIdx.x);
     // near pairs in FP64: a Boltzmann factor turns an energy error dE into a
     // relative weight error dE / T, so Widom energies get the tighter mode
-    process_cta<PointPolicy<kHenryP>, PREC_NEAR64>(s, pol, task.fw, task.cc);
+    process_cta<PointPolicy<P>, PREC_NEAR64>(s, pol, task.fw, task.cc);
 }
 
 __device__ __forceinline__ Lse lse_merge(Lse a, Lse b) {
@@ -275,8 +297,10 @@ __device__ __forceinline__ Lse lse_tree(Lse v, Lse* sm) {
 }
 
 // Block b sums insertions [b*chunk, (b+1)*chunk) (thread t: b*chunk + t + 256 k).
+// neg_inv_t = -1 / T: the exponent -E / T of src/doHenry.h:107 as a product
+// (within an ulp of the quotient; the Boltzmann factor moves by ~1e-15 relative).
 __global__ void __launch_bounds__(256) henry_reduce_kernel(const float* __restrict__ E, int n,
-                                                           double T, int chunk,
+                                                           double neg_inv_t, int chunk,
                                                            Lse* __restrict__ part) {
     __shared__ Lse sm[256];
     const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
@@ -285,7 +309,7 @@ __global__ void __launch_bounds__(256) henry_reduce_kernel(const float* __restri
         const float ef = E[i];
         if (isinf(ef)) continue;  // blocked insertion: weight 0
         const double e = (double)ef;
-        const double x = -e / T;  // src/doHenry.h:107, exp(-energy / T)
+        const double x = e * neg_inv_t;
         if (x > acc.m) {
             const double f = exp(acc.m - x);
             acc.s = acc.s * f + 1.0;
@@ -330,7 +354,8 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
     BinGeom g;
     {
         const double L0 = fw.cell_len[0], L1 = fw.cell_len[1], L2 = fw.cell_len[2];
-        const double scale = cbrt((double)n / (4.0 * kHenryP) / (L0 * L1 * L2));
+        const double scale =
+            cbrt((double)n / (4.0 * henry_points_per_thread(n)) / (L0 * L1 * L2));
         const double L[3] = {L0, L1, L2};
         int64_t nk = 8;
         for (int d = 0; d < 3; ++d) {
@@ -374,26 +399,27 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         }
     }
     int* counts = (int*)hs.counts.ptr;
-    int* fill = counts + g.n_keys;
+    int* tsum = counts + g.n_keys;  // tile sums of the scan
     int* starts = (int*)hs.starts.ptr;
     int* nblk = (int*)hs.nblk.ptr;
     float* E = (float*)hs.e.ptr;
-    ER_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * (size_t)g.n_keys * sizeof(int), st));
+    ER_CUDA(ctx, cudaMemsetAsync(counts, 0, (size_t)g.n_keys * sizeof(int), st));
     ER_CUDA(ctx, cudaMemsetAsync(nblk, 0, sizeof(int), st));
     const int gthreads = 256;
     const int gblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads,
                                                (int64_t)ctx->num_sms * 32);
+    // the slot of each insertion in its bin goes to `order` until the sort
+    // overwrites it with the sorted insertion indices
+    int* slot = (int*)hs.order.ptr;
     henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
-                                                   (int*)hs.bin.ptr, counts, E, nblk);
+                                                   (int*)hs.bin.ptr, slot, counts, E, nblk);
     {
         const int tiles = (g.n_keys + kScanTile - 1) / kScanTile;
-        int* tsum = fill;  // the fill counters are zeroed after the scan
         scan_tiles_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum);
         scan_top_kernel<<<1, 1024, 0, st>>>(tsum, tiles, starts + g.n_keys);
         scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum, starts);
-        ER_CUDA(ctx, cudaMemsetAsync(fill, 0, (size_t)g.n_keys * sizeof(int), st));
     }
-    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, n, starts, fill,
+    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, slot, n, starts,
                                                        (int*)hs.tmp.ptr);
     henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
                                                               (const int*)hs.tmp.ptr, seed,
@@ -407,17 +433,25 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
     task.order = (const int*)hs.order.ptr;
     task.n_valid = starts + g.n_keys;
     task.energies = E;
-    ER_CUDA(ctx, cudaFuncSetAttribute(henry_energy_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(EngineSmem)));
-    const int per_cta = kWarps * 32 * kHenryP;
+    const int hp = henry_points_per_thread(n);
+    const int per_cta = kWarps * 32 * hp;
     const int ecta = (n + per_cta - 1) / per_cta;
-    henry_energy_kernel<<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
+    if (hp == kHenryP) {
+        ER_CUDA(ctx, cudaFuncSetAttribute(henry_energy_kernel<kHenryP>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(EngineSmem)));
+        henry_energy_kernel<kHenryP><<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
+    } else {
+        ER_CUDA(ctx, cudaFuncSetAttribute(henry_energy_kernel<kHenryPSmall>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sizeof(EngineSmem)));
+        henry_energy_kernel<kHenryPSmall><<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
+    }
     ER_CUDA(ctx, cudaGetLastError());
     const int rblocks = std::min(4096, std::max(1, ctx->num_sms * 4));
     const int chunk = (n + rblocks - 1) / rblocks;
     const int nrb = (n + chunk - 1) / chunk;
-    henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, temperature, chunk, (Lse*)hs.part.ptr);
+    henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, -1.0 / temperature, chunk, (Lse*)hs.part.ptr);
     henry_final_kernel<<<1, 256, 0, st>>>((const Lse*)hs.part.ptr, nrb, (Lse*)hs.res.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     if (host_out) {
