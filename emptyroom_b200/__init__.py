@@ -247,6 +247,23 @@ class Context:
                                         ER_OUT_DEVICE | ER_COUNT_PAIRS,
                                         ctypes.c_void_p(int(out_ptr))))
 
+    def set_timing(self, on=True):
+        """Record per-stage device times of er_henry calls (CUDA events)."""
+        self._check(_capi.lib().er_ctx_set_timing(self._h, int(bool(on))))
+
+    def henry_timing(self):
+        """Stage times (ms) of the last timed er_henry call: bin, sort, energy, reduce."""
+        t = _capi.ErHenryTiming()
+        self._check(_capi.lib().er_henry_last_timing(self._h, ctypes.byref(t)))
+        return {"bin_ms": t.bin_ms, "sort_ms": t.sort_ms, "energy_ms": t.energy_ms,
+                "reduce_ms": t.reduce_ms}
+
+    def rcp64_seed_error(self):
+        """Largest relative error of the hardware FP64 reciprocal seed."""
+        v = ctypes.c_double(0.0)
+        self._check(_capi.lib().er_probe_rcp64_seed(self._h, ctypes.byref(v)))
+        return v.value
+
     def fp32_rate(self, seconds=0.2):
         """Measured FP32 FMA issue rate of the device (lane-instructions/s)."""
         v = ctypes.c_double(0.0)

@@ -53,6 +53,11 @@ class ErHenryResult(ctypes.Structure):
                 ("mean_energy", c_double), ("kh_mol_m3_pa", c_double)]
 
 
+class ErHenryTiming(ctypes.Structure):
+    _fields_ = [("bin_ms", c_double), ("sort_ms", c_double), ("energy_ms", c_double),
+                ("reduce_ms", c_double)]
+
+
 class ErJob(ctypes.Structure):
     _fields_ = [("kind", c_int), ("fw_key", c_uint64), ("desc", c_void_p), ("nx", c_int),
                 ("ny", c_int), ("nz", c_int), ("temperature", c_double),
@@ -93,6 +98,8 @@ SIGNATURES = {
                                c_int, c_int, c_int, ctypes.POINTER(ErHenryResult), _ip]),
     "er_henry_stats_noalloc": (c_int, [c_void_p, c_void_p, c_int64, c_double,
                                        ctypes.POINTER(ErHenryResult)]),
+    "er_ctx_set_timing": (c_int, [c_void_p, c_int]),
+    "er_henry_last_timing": (c_int, [c_void_p, ctypes.POINTER(ErHenryTiming)]),
     "er_block_pockets": (c_int, [c_void_p, _dp, c_int, c_int, c_int, c_double, _ip, _ip]),
     "er_block_pockets_device": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_double,
                                         c_void_p, _ip]),
@@ -138,6 +145,7 @@ SIGNATURES = {
                                  c_size_t]),
     "er_version": (ctypes.c_char_p, []),
     "er_probe_fp32_rate": (c_int, [c_void_p, c_double, _dp]),
+    "er_probe_rcp64_seed": (c_int, [c_void_p, _dp]),
 }
 
 _lib = None

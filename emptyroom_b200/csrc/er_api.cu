@@ -88,6 +88,14 @@ int set_error(er_ctx* ctx, int status, const std::string& msg) {
     return status;
 }
 
+int take_fault(er_ctx* ctx) {
+    if (!ctx->fault_host || !*(volatile int*)ctx->fault_host) return ER_OK;
+    *(volatile int*)ctx->fault_host = 0;
+    return set_error(ctx, ER_ERR_CUDA,
+                     "engine: a bounded wait for staged atom images gave up; the grid points "
+                     "or insertions of the affected blocks were not written");
+}
+
 int cuda_error(er_ctx* ctx, cudaError_t e, const char* what) {
     std::string m = std::string(what) + ": " + cudaGetErrorString(e);
     cudaGetLastError();
@@ -432,7 +440,19 @@ int er_ctx_create(int device, er_ctx** out) {
         }
     }
     int st = configure_kernels(ctx);
+    if (st == ER_OK) {
+        if (cudaHostAlloc((void**)&ctx->fault_host, sizeof(int), cudaHostAllocMapped) !=
+                cudaSuccess ||
+            cudaHostGetDevicePointer((void**)&ctx->fault_dev, ctx->fault_host, 0) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            st = ER_ERR_CUDA;
+        } else {
+            *ctx->fault_host = 0;
+        }
+    }
     if (st != ER_OK) {
+        if (ctx->fault_host) cudaFreeHost(ctx->fault_host);
         cudaMemPoolDestroy(ctx->pool);
         cudaStreamDestroy(ctx->copy_stream);
         cudaStreamDestroy(ctx->stream);
@@ -466,12 +486,15 @@ void er_ctx_destroy(er_ctx* ctx) {
     }
     ctx->pipes.clear();
     ctx->henry.release();
+    for (cudaEvent_t& e : ctx->henry.ev)
+        if (e) cudaEventDestroy(e);
     ctx->pinned.release();
     ctx->plan_pinned.release();
     ctx->task_left.release();
     cudaStreamSynchronize(ctx->stream);
     cudaMemPoolDestroy(ctx->pool);
     if (ctx->done_host) cudaFreeHost(ctx->done_host);
+    if (ctx->fault_host) cudaFreeHost(ctx->fault_host);
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
     cudaStreamDestroy(ctx->stream);
@@ -482,7 +505,7 @@ const char* er_ctx_last_error(const er_ctx* ctx) { return ctx ? ctx->last_error.
 
 int er_ctx_synchronize(er_ctx* ctx) {
     if (!ctx) return ER_ERR_INVALID;
-    ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ER_SYNC(ctx, ctx->stream);
     return ER_OK;
 }
 
@@ -554,6 +577,7 @@ void fw_record(const HostFramework& hf, size_t n_img, const FwLayout& L, void* b
     for (int k = 0; k < 9; ++k) d.r[k] = hf.r[k];
     d.rc2 = hf.rc2;
     d.imgs_per_atom = hf.imgs_per_atom;
+    d.fault = nullptr;
     rec.bytes = L.total;
     rec.rc2 = hf.rc2;
     for (int k = 0; k < 9; ++k) rec.t[k] = hf.t[k];
@@ -640,6 +664,7 @@ int host_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* fw
     for (int i = 0; i < n; ++i) {
         FwRecord rec;
         fw_record(hfs[i], hfs[i].img_xyz.size(), lay[i], blocks[i], rec);
+        rec.dev.fault = ctx->fault_dev;
         const int id = ctx->next_fw++;
         ctx->fws[id] = rec;
         fw_ids[i] = id;
@@ -707,7 +732,7 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
         if (!dev_out) {
             ER_CUDA(ctx, cudaMemcpyAsync(out, d64, npts * sizeof(double), cudaMemcpyDeviceToHost,
                                          ctx->stream));
-            ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            ER_SYNC(ctx, ctx->stream);
         }
         return ER_OK;
     }
@@ -731,13 +756,13 @@ int er_grid(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int flags, void* out
         if (!f64) {
             ER_CUDA(ctx, cudaMemcpyAsync(out, dst, npts * sizeof(float), cudaMemcpyDeviceToHost,
                                          ctx->stream));
-            ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            ER_SYNC(ctx, ctx->stream);
         } else {
             // D2H as float (half the bytes), widen on the host
             float* tmp = (float*)out;  // the first half of the caller's double buffer
             ER_CUDA(ctx, cudaMemcpyAsync(tmp, dst, npts * sizeof(float), cudaMemcpyDeviceToHost,
                                          ctx->stream));
-            ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            ER_SYNC(ctx, ctx->stream);
             double* o = (double*)out;
             for (size_t i = npts; i-- > 0;) o[i] = (double)tmp[i];
         }
@@ -766,7 +791,7 @@ int er_grid_sheet(er_ctx* ctx, int fw_id, int nx, int ny, int nz, int x_index,
         return set_error(ctx, ER_ERR_NOMEM, "sheet: pinned staging failed");
     ER_CUDA(ctx, cudaMemcpyAsync(ctx->pinned.ptr, (float*)c.grid.ptr + (size_t)x_index * ns,
                                  ns * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-    ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ER_SYNC(ctx, ctx->stream);
     const float* src = (const float*)ctx->pinned.ptr;
     for (size_t i = 0; i < ns; ++i) out_sheet[i] = (double)src[i];
     return ER_OK;
@@ -1070,7 +1095,7 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->copy_stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "batch: run / copy-out");
-        return ER_OK;
+        return take_fault(ctx);
     }
     er_batch_plan* p = nullptr;
     int st = er_batch_plan_create(ctx, jobs, n_jobs, mode, &p);
@@ -1078,6 +1103,7 @@ int er_grid_batch(er_ctx* ctx, const er_grid_job* jobs, int n_jobs, int mode) {
     st = er_batch_plan_run(p);
     if (st == ER_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         st = cuda_error(ctx, cudaGetLastError(), "batch: run");
+    if (st == ER_OK) st = take_fault(ctx);
     er_batch_plan_destroy(p);
     return st;
 }
@@ -1107,6 +1133,44 @@ __global__ void __launch_bounds__(256) fp32_rate_kernel(int iters, float seed, f
 }
 
 }  // namespace er
+
+// Largest |1 - x y0| over `per_thread` samples per thread of y0 =
+// rcp.approx.ftz.f64(x), x = m 2^k with m uniform in [1, 2) (Philox stream 7)
+// and k in [-80, 20) (the squared distances the near pairs can see). The
+// residual is formed by one FMA, exact up to its final rounding.
+__global__ void __launch_bounds__(256) rcp64_seed_kernel(int per_thread,
+                                                         unsigned long long* max_bits) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double worst = 0.0;
+    for (int i = 0; i < per_thread; ++i) {
+        double f[3];
+        insertion_point(7, tid * (uint64_t)per_thread + (uint64_t)i, f);
+        const int k = (int)(f[1] * 100.0) - 80;
+        const double x = ldexp(1.0 + f[0], k);
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+        worst = fmax(worst, fabs(fma(-x, y, 1.0)));
+    }
+    atomicMax(max_bits, (unsigned long long)__double_as_longlong(worst));
+}
+
+extern "C" int er_probe_rcp64_seed(er_ctx* ctx, double* max_rel_err) {
+    if (!ctx || !max_rel_err) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->counter.ensure(4096 * sizeof(float)) != ER_OK)
+        return set_error(ctx, ER_ERR_NOMEM, "probe: allocation failed");
+    unsigned long long* bits = (unsigned long long*)ctx->counter.ptr;
+    ER_CUDA(ctx, cudaMemsetAsync(bits, 0, sizeof(*bits), ctx->stream));
+    rcp64_seed_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(64, bits);
+    ER_CUDA(ctx, cudaGetLastError());
+    unsigned long long h = 0;
+    ER_CUDA(ctx, cudaMemcpyAsync(&h, bits, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    ER_SYNC(ctx, ctx->stream);
+    double v;
+    memcpy(&v, &h, sizeof(v));
+    *max_rel_err = v;
+    return ER_OK;
+}
 
 extern "C" int er_probe_fp32_rate(er_ctx* ctx, double seconds, double* instr_per_s) {
     if (!ctx || !instr_per_s || !(seconds > 0)) return ER_ERR_INVALID;

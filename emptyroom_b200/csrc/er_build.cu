@@ -490,6 +490,7 @@ int device_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* 
     for (int i = 0; i < n; ++i) {
         FwRecord rec;
         fw_record(hfs[i], h_cnt[i], lay[i], blocks[i], rec);
+        rec.dev.fault = ctx->fault_dev;
         const int id = ctx->next_fw++;
         ctx->fws[id] = rec;
         fw_ids[i] = id;

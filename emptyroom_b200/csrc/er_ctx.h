@@ -52,6 +52,9 @@ struct HostBuf {
 // runs Widom jobs concurrently.
 struct HenryScratch {
     DevBuf pts, bin, order, tmp, counts, starts, e, nblk, part, res, mask;
+    // stage boundaries of the last run (er_ctx_set_timing): start, binned,
+    // sorted, energies, reduced; ev[0] == nullptr while timing is off
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     size_t bytes() const {
         return pts.cap + bin.cap + order.cap + tmp.cap + counts.cap + starts.cap + e.cap +
                nblk.cap + part.cap + res.cap + mask.cap;
@@ -108,6 +111,8 @@ struct er_ctx {
     er::HostBuf plan_pinned; // pinned staging of batch-plan queues
     cudaMemPool_t pool = nullptr;  // stream-ordered pool (framework blocks, plan queues)
     er::DevBuf task_left;    // per-job bricks left (completion notification)
+    int* fault_host = nullptr;  // mapped pinned word a kernel sets when a bounded wait
+    int* fault_dev = nullptr;   // gives up (FwDev::fault of every framework), its device address
     int* done_host = nullptr;   // mapped pinned per-job completion flags
     int* done_dev = nullptr;    // the same flags, device address
     size_t done_cap = 0;
@@ -164,6 +169,9 @@ int set_error(er_ctx* ctx, int status, const std::string& msg);
 // keeps freed memory for reuse (trimmed and retried once when exhausted).
 int pool_alloc(er_ctx* ctx, void** p, size_t bytes);
 int cuda_error(er_ctx* ctx, cudaError_t e, const char* what);
+// ER_ERR_CUDA (and the word cleared) when a kernel has set the context's
+// fault word since the last check, else ER_OK.
+int take_fault(er_ctx* ctx);
 const FwRecord* find_fw(er_ctx* ctx, int fw_id);
 // Cutoff constants for a framework and a CTA box diagonal (A).
 CutoffConsts make_cutoff_consts(double rc2, double box_diag, double r2min);
@@ -203,4 +211,12 @@ int device_upload_many(er_ctx* ctx, const er_framework_desc* descs, int n, int* 
     do {                                                        \
         cudaError_t _e = (call);                                \
         if (_e != cudaSuccess) return er::cuda_error(ctx, _e, #call); \
+    } while (0)
+
+// Synchronises `stream`, then reports a fault a kernel raised in the
+// context's fault word (a bounded wait that gave up) as ER_ERR_CUDA.
+#define ER_SYNC(ctx, stream)                                    \
+    do {                                                        \
+        ER_CUDA(ctx, cudaStreamSynchronize(stream));            \
+        if (int _f = er::take_fault(ctx)) return _f;            \
     } while (0)

@@ -39,6 +39,7 @@
 #include <stdint.h>
 
 #include "er_internal.h"
+#include "er_philox.h"
 
 namespace er {
 
@@ -103,6 +104,7 @@ struct __align__(32) EngineSmem {
     double box[6];                         // CTA box (FP64 lo, hi)
     float wbox[kWarps][6];                 // warp boxes (local FP32 lo, hi)
     int item, task;                        // persistent-queue item and its task
+    unsigned long long mbar[2];            // completion barriers of the staged cell rows
 };
 
 // ----------------------------------------------------------- packed FP32x2
@@ -147,6 +149,50 @@ __device__ __forceinline__ float rcp_approx(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
+}
+
+// ------------------------------------------------ bulk copies (TMA engine)
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// the single arrival of a phase, announcing the bytes the phase's copies bring
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// Waits for the phase of `parity` to complete; false after kMbarSpins polls
+// (a copy that never lands: the caller records the fault instead of hanging).
+constexpr int kMbarSpins = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = smem_u32(bar);
+    for (int i = 0; i < kMbarSpins; ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// global -> shared copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) by the bulk-copy engine, completing on `bar`; one CTA, no multicast
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // Exclusive block scan of one int per thread; *total gets the block sum.
@@ -230,25 +276,29 @@ __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, 
     const double u3 = u * u * u;
     return u3 * fma(a.c12, u3, -a.c6);
 }
-// 1/x in FP64 for the near pairs of PREC_NEAR64 by Newton's method for the
-// reciprocal: from the hardware seed y0 = rcp.approx.ftz.f64(x) (relative
-// error e0 < 2^-16), one third-order step y = y0 (1 + e + e^2), e = 1 - x y0,
-// leaves a relative error of order e0^3 plus a few FP64 roundings, i.e.
-// within a few ulps of 1/x. x is a squared distance, clamped to >= min_r^2 >
-// 0 by the caller, so the seed is finite and normal.
+// 1/x in FP64 for the near pairs of PREC_NEAR64: one Newton step
+// y = y0 (1 + e), e = 1 - x y0, from the hardware seed y0 =
+// rcp.approx.ftz.f64(x), whose relative error e0 is below 2^-16 (measured by
+// er_probe_rcp64_seed, asserted by the tests), leaves a relative error of
+// order e0^2 < 2^-32 plus two FP64 roundings. A near term then carries at
+// most ~6 x 2^-32 of its own size, far below the 1e-5 relative bound on the
+// energy even where near terms cancel a thousandfold (a third-order step,
+// e0^3, gave the same errors on 71,378 sampled E < -10 K points of the
+// 256-framework batch and took 0.8 % longer). x is a squared distance,
+// clamped to >= min_r^2 > 0 by the caller, so the seed is finite and normal.
 __device__ __forceinline__ double rcp64_nr(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     const double e = fma(-x, y, 1.0);
-    return fma(y, fma(e, e, e), y);
+    return fma(y, e, y);
 }
-// FP64 pair term of a near pair (PREC_NEAR64): r^2 from dx and the shared
-// dy^2 + dz^2, reciprocal by rcp64_nr.
-__device__ __forceinline__ double near_term64(double dx, double yz, double c12, double c6,
-                                              double r2min) {
+// acc + the FP64 pair term of a near pair (PREC_NEAR64): r^2 from dx and the
+// shared dy^2 + dz^2, reciprocal by rcp64_nr, the term added by one FMA.
+__device__ __forceinline__ double near_acc64(double acc, double dx, double yz, double c12,
+                                             double c6, double r2min) {
     const double u = rcp64_nr(fmax(fma(dx, dx, yz), r2min));
     const double u3 = u * u * u;
-    return u3 * fma(c12, u3, -c6);
+    return fma(u3, fma(c12, u3, -c6), acc);
 }
 
 // FP32 r^2 of the generic form (each point has its own x, y, z) and of the
@@ -317,11 +367,21 @@ struct GridPolicy {
         f[2] = __ddiv_rn((double)k, (double)(T->nz - 1));
         return ok;
     }
+    // the point's Cartesian position in the positioning frame r
+    __device__ __forceinline__ bool cart(const double* r, int w, int lane, int p, double& x,
+                                         double& y, double& z) const {
+        double f[3];
+        const bool ok = point(w, lane, p, f);
+        frac_to_cart(r, f[0], f[1], f[2], x, y, z);
+        return ok;
+    }
     __device__ __forceinline__ void store(int w, int lane, int p, float e) const {
         int i, j, k;
         index(w, lane, p, i, j, k);
         if (i < T->nx && j < T->ny && k < T->nz)
-            T->out[(size_t)k + (size_t)j * T->nz + (size_t)i * T->ny * T->nz] = e;
+            // streaming store: the grid is written once and not read back here,
+            // so its lines are the first the L2 evicts
+            __stcs(&T->out[(size_t)k + (size_t)j * T->nz + (size_t)i * T->ny * T->nz], e);
     }
     __device__ __forceinline__ void store64(int w, int lane, int p, double e) const {
         int i, j, k;
@@ -346,13 +406,27 @@ struct PointPolicy {
         const int pos = base + w * (32 * kP) + p * 32 + lane;
         return pos < nv ? T->order[pos] : -1;
     }
+    __device__ __forceinline__ int pos_of(int w, int lane, int p, bool& ok) const {
+        const int pos = base + w * (32 * kP) + p * 32 + lane;
+        ok = pos < nv;
+        return ok ? pos : min(base, nv - 1);  // a finite stand-in, never stored
+    }
+    // Cartesian position (frame r), stored in sorted order by the bin sort
+    __device__ __forceinline__ bool cart(const double*, int w, int lane, int p, double& x,
+                                         double& y, double& z) const {
+        bool ok;
+        const int pos = pos_of(w, lane, p, ok);
+        x = T->pts[3 * (size_t)pos];
+        y = T->pts[3 * (size_t)pos + 1];
+        z = T->pts[3 * (size_t)pos + 2];
+        return ok;
+    }
+    // fractional position, regenerated from the insertion's Philox counter
+    // (only the exact cutoff decisions need it)
     __device__ __forceinline__ bool point(int w, int lane, int p, double* f) const {
-        int pos = base + w * (32 * kP) + p * 32 + lane;
-        const bool ok = pos < nv;
-        if (!ok) pos = min(base, nv - 1);  // a finite stand-in, never stored
-        f[0] = T->pts[3 * (size_t)pos];
-        f[1] = T->pts[3 * (size_t)pos + 1];
-        f[2] = T->pts[3 * (size_t)pos + 2];
+        bool ok;
+        const int pos = pos_of(w, lane, p, ok);
+        insertion_point(T->seed, (uint64_t)T->order[pos], f);
         return ok;
     }
     __device__ __forceinline__ void store(int w, int lane, int p, float e) const {
@@ -864,9 +938,8 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
     // FP64 positions of this lane's points relative to the CTA centre
     // (FP64 paths only).
     auto point64 = [&](int p, double& qx, double& qy, double& qz) {
-        double f[3], x, y, z, o0, o1, o2;
-        pol.point(w, lane, p, f);
-        frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
+        double x, y, z, o0, o1, o2;
+        pol.cart(fw.r, w, lane, p, x, y, z);
         cta_centre(s, o0, o1, o2);
         qx = x - o0;
         qy = y - o1;
@@ -963,13 +1036,13 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
                     const double yz = fma(dz, dz, dy * dy);
 #pragma unroll
                     for (int p = 0; p < kNearP; ++p)
-                        nacc[p] += near_term64(qx[p] - a.x, yz, a.c12, a.c6, cc.r2min);
+                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x, yz, a.c12, a.c6, cc.r2min);
                 } else {
 #pragma unroll
                     for (int p = 0; p < kNearP; ++p) {
                         const double dy = qy[p] - a.y, dz = qz[p] - a.z;
-                        nacc[p] += near_term64(qx[p] - a.x, fma(dz, dz, dy * dy), a.c12, a.c6,
-                                               cc.r2min);
+                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x, fma(dz, dz, dy * dy), a.c12,
+                                             a.c6, cc.r2min);
                     }
                 }
             }
@@ -998,7 +1071,7 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
                     if (inside) {
                         const double u = rcp64_nr(r2);
                         const double u3 = u * u * u;
-                        nacc[p] += u3 * fma(a.c12, u3, -a.c6);
+                        nacc[p] = fma(u3, fma(a.c12, u3, -a.c6), nacc[p]);
                     }
                 }
             }
@@ -1013,7 +1086,9 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
 // live in registers through the pair loops (at the 80-register limit of three
 // CTAs per SM that took the 256-framework batch from 370 to 357 ms). The
 // Widom kernel (128 registers, generic points) is faster with the flush
-// inlined (1.89 against 2.18 ms per 1e7 insertions).
+// inlined: 1.28 ms per 1e7 insertions against 1.61 ms out of line; out of
+// line at 80 registers and three CTAs per SM (P = 4, 6 or 8) it took
+// 1.42-1.51 ms.
 template <class Pol, int PREC>
 static __device__ __noinline__ void warp_flush_call(EngineSmem& s, const Pol& pol,
                                                     const FwDev& fw, const CutoffConsts& cc,
@@ -1044,9 +1119,8 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     double mx0 = -INFINITY, mx1 = -INFINITY, mx2 = -INFINITY;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        double f[3], x, y, z;
-        const bool ok = pol.point(w, lane, p, f);
-        frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
+        double x, y, z;
+        const bool ok = pol.cart(fw.r, w, lane, p, x, y, z);
         if (ok) {
             L.vmask |= 1u << p;
             mn0 = fmin(mn0, x); mn1 = fmin(mn1, y); mn2 = fmin(mn2, z);
@@ -1092,9 +1166,8 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
         float wh0x = -INFINITY, wh0y = -INFINITY, wh0z = -INFINITY;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            double f[3], x, y, z;
-            pol.point(w, lane, p, f);
-            frac_to_cart(fw.r, f[0], f[1], f[2], x, y, z);
+            double x, y, z;
+            pol.cart(fw.r, w, lane, p, x, y, z);
             const float fx = (float)(x - o0), fy = (float)(y - o1), fz = (float)(z - o2);
             L.px[p] = fx;
             if (!Pol::kLattice || p == 0) {
@@ -1123,6 +1196,30 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
         __syncwarp();
     }
 
+// ER_BULK=1 (a build option: `make -C emptyroom_b200/csrc clean all cli
+// ER_BULK=1`) selects the producer whose cell-row image ranges arrive in
+// shared memory by bulk copies of the TMA engine (cp.async.bulk, 256 images per stage, two stages in flight, each
+// completing on an mbarrier). Measured on the 256-framework batch it is
+// slower than the default producer (per-thread loads of the same images):
+// 382.8 against 373.6 ms in the default mode, 311.3 against 303.1 ms in
+// ER_PREC_COMP, the Widom energy kernel 1.296 against 1.278 ms per 1e7
+// insertions -- each stage adds a block-wide wait, and the staging state
+// raises the producer's register spills (grid_persistent_kernel<3>: 364 /
+// 1000 bytes of spill stores / loads against 280 / 584).
+#ifndef ER_BULK
+#define ER_BULK 0
+#endif
+#if ER_BULK
+    // staging barriers of this pass (initialised here, invalidated at its end)
+    if (tid == 0) {
+        mbar_init(&s.mbar[0]);
+        mbar_init(&s.mbar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+#endif
+    unsigned mph = 0;    // phase parity of each staging barrier
+    bool fault = false;  // a staging wait gave up
     // 3. producer: rows of cells around the CTA box, streamed into shared memory
     const double R = cc.rcm, R2 = R * R;
     const float R2f = (float)R2;
@@ -1168,6 +1265,75 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
             s.row_off[tid] = off;
             __syncthreads();
             const int nr = min(kRowChunk, nrows - rb);
+#if ER_BULK
+            // the rows' image ranges arrive by bulk copies, kThreads images
+            // per stage, two stages in flight in the staging area (the per-warp
+            // lists, unused while the producer runs)
+            double4* stg = reinterpret_cast<double4*>(&s.wl[0][0]);
+            const int nst = (tot + kThreads - 1) / kThreads;
+            auto issue = [&](int k) {
+                const int b = k & 1;
+                const int lo = k * kThreads, hi = min(tot, lo + kThreads);
+                if (tid == 0) mbar_expect_tx(&s.mbar[b], (unsigned)(hi - lo) * 32u);
+                const int a = max(lo, off), e = min(hi, off + len);
+                if (a < e)
+                    bulk_g2s(stg + b * kThreads + (a - lo), fw.img_xyz + beg + (a - off),
+                             (unsigned)(e - a) * 32u, &s.mbar[b]);
+            };
+            if (nst > 0) issue(0);
+            for (int k = 0; k < nst; ++k) {
+                const int b = k & 1;
+                if (k + 1 < nst) issue(k + 1);
+                fault |= !mbar_wait(&s.mbar[b], (mph >> b) & 1u);
+                mph ^= 1u << b;
+                const int c = k * kThreads + tid;
+                int pass = 0, g = 0;
+                float ax = 0.f, ay = 0.f, az = 0.f, c12 = 0.f, nc6 = 0.f;
+                if (c < tot) {
+                    const double4 ap = stg[b * kThreads + tid];
+                    ax = (float)(ap.x - o0);
+                    ay = (float)(ap.y - o1);
+                    az = (float)(ap.z - o2);
+                    const float ddx = fmaxf(0.f, fmaxf(b0x - ax, ax - b1x));
+                    const float ddy = fmaxf(0.f, fmaxf(b0y - ay, ay - b1y));
+                    const float ddz = fmaxf(0.f, fmaxf(b0z - az, az - b1z));
+                    pass = (ddx * ddx + ddy * ddy + ddz * ddz) < R2f;
+                    if (pass) {
+                        int a = 0, bb = nr - 1;
+                        while (a < bb) {
+                            const int mid = (a + bb + 1) >> 1;
+                            if (s.row_off[mid] <= c) a = mid; else bb = mid - 1;
+                        }
+                        g = s.row_beg[a] + (c - s.row_off[a]);
+                        const float2 pr = fw.img_par[g];
+                        c12 = pr.x;
+                        nc6 = pr.y;
+                    }
+                }
+                int npass;
+                const int pos = block_exscan(pass, s.warp_tot, &npass);
+                if (n_cand + npass > kMaxCand) {
+                    // the flush writes the staging area: the next stage lands
+                    // first and is copied again after it
+                    if (k + 1 < nst) {
+                        fault |= !mbar_wait(&s.mbar[b ^ 1], (mph >> (b ^ 1)) & 1u);
+                        mph ^= 1u << (b ^ 1);
+                    }
+                    __syncthreads();
+                    warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, L);
+                    __syncthreads();
+                    n_cand = 0;
+                    if (k + 1 < nst) issue(k + 1);
+                }
+                if (pass) {
+                    Cand& dst = s.cand[n_cand + pos];
+                    *reinterpret_cast<float4*>(&dst.ax) = make_float4(ax, ax, ay, az);
+                    *reinterpret_cast<float4*>(&dst.c12) = make_float4(c12, c12, nc6, nc6);
+                    s.cid[n_cand + pos] = g;
+                }
+                n_cand += npass;
+            }
+#else
             for (int cb = 0; cb < tot; cb += kThreads) {
                 const int c = cb + tid;
                 int pass = 0, g = 0;
@@ -1209,6 +1375,7 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
                 }
                 n_cand += npass;
             }
+#endif
             __syncthreads();
         }
     }
@@ -1216,7 +1383,18 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
         __syncthreads();
         warp_flush<Pol, PREC>(s, pol, fw, cc, n_cand, L);
     }
-    // 4. store
+    // 4. store (nothing when a staging wait gave up: the pass is reported
+    // through the fault word instead of storing energies of missing atoms)
+    if (__syncthreads_or(fault)) {
+        if (tid == 0 && fw.fault) atomicExch(fw.fault, 1);
+        L.vmask = 0;
+    }
+#if ER_BULK
+    if (tid == 0) {
+        mbar_inval(&s.mbar[0]);
+        mbar_inval(&s.mbar[1]);
+    }
+#endif
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         if (L.vmask & (1u << p)) {

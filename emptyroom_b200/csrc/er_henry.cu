@@ -233,12 +233,19 @@ __global__ void henry_scatter_kernel(const int* __restrict__ key, const int* __r
     }
 }
 
+// The positioning frame r of a framework, by value.
+struct Frame {
+    double r[9];
+};
+
 // One warp per bin: rank of each entry among its bin's entries -> ascending
 // order (the bin's entries compared 32 at a time through shuffles); the
 // insertion point itself (recomputed from its Philox counter) is written in the
-// same sorted order, so the energy kernel reads it coalesced.
+// same sorted order as its Cartesian position in frame r (the engine's own
+// frac_to_cart, so the bits are those the engine would compute), which the
+// energy kernel reads coalesced.
 __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_keys,
-                                       const int* __restrict__ tmp, uint64_t seed,
+                                       const int* __restrict__ tmp, uint64_t seed, Frame fr,
                                        int* __restrict__ order, double* __restrict__ pts_sorted) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -255,11 +262,12 @@ __global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_key
             }
             if (q < L) {
                 order[s + rank] = v;
-                double f[3];
+                double f[3], x, y, z;
                 insertion_point(seed, (uint64_t)v, f);
-                pts_sorted[3 * (size_t)(s + rank)] = f[0];
-                pts_sorted[3 * (size_t)(s + rank) + 1] = f[1];
-                pts_sorted[3 * (size_t)(s + rank) + 2] = f[2];
+                frac_to_cart(fr.r, f[0], f[1], f[2], x, y, z);
+                pts_sorted[3 * (size_t)(s + rank)] = x;
+                pts_sorted[3 * (size_t)(s + rank) + 1] = y;
+                pts_sorted[3 * (size_t)(s + rank) + 2] = z;
             }
         }
     }
@@ -411,6 +419,7 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
     // the slot of each insertion in its bin goes to `order` until the sort
     // overwrites it with the sorted insertion indices
     int* slot = (int*)hs.order.ptr;
+    if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[0], st));
     henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
                                                    (int*)hs.bin.ptr, slot, counts, E, nblk);
     {
@@ -419,18 +428,23 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         scan_top_kernel<<<1, 1024, 0, st>>>(tsum, tiles, starts + g.n_keys);
         scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum, starts);
     }
+    if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[1], st));
     henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, slot, n, starts,
                                                        (int*)hs.tmp.ptr);
+    Frame fr;
+    for (int k = 0; k < 9; ++k) fr.r[k] = fw.dev.r[k];
     henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
-                                                              (const int*)hs.tmp.ptr, seed,
+                                                              (const int*)hs.tmp.ptr, seed, fr,
                                                               (int*)hs.order.ptr,
                                                               (double*)hs.pts.ptr);
     ER_CUDA(ctx, cudaGetLastError());
+    if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[2], st));
     PointTask task;
     task.fw = fw.dev;
     task.cc = make_cutoff_consts(fw.rc2, 0.0, 1e-16 * 1e-16);  // min_r, src/doHenry.h:15
     task.pts = (const double*)hs.pts.ptr;
     task.order = (const int*)hs.order.ptr;
+    task.seed = seed;
     task.n_valid = starts + g.n_keys;
     task.energies = E;
     const int hp = henry_points_per_thread(n);
@@ -448,12 +462,14 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         henry_energy_kernel<kHenryPSmall><<<ecta, kThreads, sizeof(EngineSmem), st>>>(task);
     }
     ER_CUDA(ctx, cudaGetLastError());
+    if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[3], st));
     const int rblocks = std::min(4096, std::max(1, ctx->num_sms * 4));
     const int chunk = (n + rblocks - 1) / rblocks;
     const int nrb = (n + chunk - 1) / chunk;
     henry_reduce_kernel<<<nrb, 256, 0, st>>>(E, n, -1.0 / temperature, chunk, (Lse*)hs.part.ptr);
     henry_final_kernel<<<1, 256, 0, st>>>((const Lse*)hs.part.ptr, nrb, (Lse*)hs.res.ptr);
     ER_CUDA(ctx, cudaGetLastError());
+    if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[4], st));
     if (host_out) {
         ER_CUDA(ctx, cudaMemcpyAsync(host_out->lse, hs.res.ptr, sizeof(Lse),
                                      cudaMemcpyDeviceToHost, st));
@@ -510,8 +526,42 @@ extern "C" int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_in
     if (energies_out)
         ER_CUDA(ctx, cudaMemcpyAsync(energies_out, ctx->henry.e.ptr, (size_t)n_ins * sizeof(float),
                                      cudaMemcpyDeviceToHost, ctx->stream));
-    ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ER_SYNC(ctx, ctx->stream);
     henry_finish(h, n_ins, temperature, out);
+    return ER_OK;
+}
+
+extern "C" int er_ctx_set_timing(er_ctx* ctx, int on) {
+    if (!ctx) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    HenryScratch& hs = ctx->henry;
+    if (on && !hs.ev[0]) {
+        for (cudaEvent_t& e : hs.ev) ER_CUDA(ctx, cudaEventCreate(&e));
+    } else if (!on && hs.ev[0]) {
+        ER_SYNC(ctx, ctx->stream);
+        for (cudaEvent_t& e : hs.ev) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+    }
+    return ER_OK;
+}
+
+extern "C" int er_henry_last_timing(er_ctx* ctx, er_henry_timing* out) {
+    if (!ctx || !out) return ER_ERR_INVALID;
+    *out = er_henry_timing{0.0, 0.0, 0.0, 0.0};
+    const HenryScratch& hs = ctx->henry;
+    if (!hs.ev[0]) return set_error(ctx, ER_ERR_INVALID, "henry timing: timing is off");
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    float ms[4];
+    for (int k = 0; k < 4; ++k) {
+        const cudaError_t e = cudaEventElapsedTime(&ms[k], hs.ev[k], hs.ev[k + 1]);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, ER_ERR_INVALID, "henry timing: no timed er_henry call yet");
+        }
+    }
+    *out = er_henry_timing{ms[0], ms[1], ms[2], ms[3]};
     return ER_OK;
 }
 
@@ -550,7 +600,7 @@ int henry_one(er_ctx* ctx, HenryPipe& P, const FwRecord& fw, double temperature,
     int s = henry_enqueue(ctx, fw, temperature, (int)n_ins, seed, mask, bd[0], bd[1], bd[2], st,
                           P.hs, P.out);
     if (s != ER_OK) return s;
-    ER_CUDA(ctx, cudaStreamSynchronize(st));
+    ER_SYNC(ctx, st);
     henry_finish(*P.out, n_ins, temperature, out);
     if (n_pockets) *n_pockets = npk;
     return ER_OK;
@@ -627,5 +677,5 @@ extern "C" int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temp
         cudaStreamSynchronize(ctx->pipes[p]->stream);
         if (status[p] != ER_OK) return status[p];
     }
-    return ER_OK;
+    return take_fault(ctx);
 }

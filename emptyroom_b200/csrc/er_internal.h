@@ -32,6 +32,8 @@ struct FwDev {
     double rc2;               // squared cutoff, FP64 (the reference's r_cutoff_squared)
     int rep[3];
     int imgs_per_atom;        // (2 rep0 + 1)(2 rep1 + 1)(2 rep2 + 1)
+    int* fault;               // set to 1 by a kernel whose bounded wait gave up (the
+                              // context's mapped fault word; may be null)
 };
 
 // Per-launch constants derived from the cutoff.
@@ -61,8 +63,11 @@ struct GridTask {
 struct PointTask {
     FwDev fw;
     CutoffConsts cc;
-    const double* pts;       // FP64 fractional points, 3 per entry of `order` (bin order)
+    const double* pts;       // FP64 Cartesian points (frame r), 3 per entry of `order`
+                             // (bin order)
     const int* order;        // unblocked insertion indices in bin order
+    uint64_t seed;           // Philox stream of the points (fractional coordinates are
+                             // regenerated from it for the exact cutoff decisions)
     const int* n_valid;      // device count of entries in `order`
     float* energies;         // E per insertion (insertion order)
 };

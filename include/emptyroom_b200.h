@@ -93,8 +93,9 @@ int er_framework_bytes(er_ctx* ctx, int fw_id, size_t* bytes);
 #define ER_PREC_NEAR64 0x0  /* default: FP32 pair terms except the pairs of atoms within
                                 5 A of a warp's points, which are FP64 (the large terms
                                 whose FP32 rounding dominates where terms cancel); FP32
-                                sums of 64 terms folded into FP64 per-point totals.
-                                Within 1e-5 relative of FP64 on points with E < -10 K */
+                                sums of 16 terms (64 on the cutoff shell) folded into
+                                FP64 per-point totals. Within 1e-5 relative of FP64 on
+                                points with E < -10 K */
 #define ER_PREC_COMP 0x08    /* all pair terms FP32, FP32 sums of 64 terms folded into
                                 FP64 per-point totals: faster, but its error on E < 0
                                 points reaches ~2e-5 relative where large near terms
@@ -206,6 +207,18 @@ int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t
 int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
                    int64_t n_insertions, const uint64_t* seeds, int block_nx, int block_ny,
                    int block_nz, er_henry_result* results, int* n_pockets);
+
+/* Device time (ms) of each stage of the last er_henry call on ctx, taken with
+ * CUDA events on the context stream while timing is on (er_ctx_set_timing,
+ * off by default): Philox points, mask test and bin counts; the bin sort; the
+ * Lennard-Jones energy kernel; the FP64 log-sum-exp reduction. The reference
+ * times only the whole run ("Simulation time", src/henry.cu:150-153).
+ * er_henry_batch, the server and er_henry_stats_noalloc record nothing. */
+typedef struct {
+    double bin_ms, sort_ms, energy_ms, reduce_ms;
+} er_henry_timing;
+int er_ctx_set_timing(er_ctx* ctx, int on);
+int er_henry_last_timing(er_ctx* ctx, er_henry_timing* out);
 
 /* Widom statistics of energies the caller already holds on the device,
  * computed without allocating anything: no counterpart in the reference.
@@ -442,6 +455,12 @@ int er_read_grid_txt(const char* path, double* out, size_t cap, int dims[3], cha
  * (FP32-pipe lane-instructions per second, whole GPU) over about `seconds`.
  * This is the denominator of the pair-sum roofline. */
 int er_probe_fp32_rate(er_ctx* ctx, double seconds, double* instr_per_s);
+
+/* Largest relative error |1 - x y0| of the hardware FP64 reciprocal seed y0
+ * (rcp.approx.ftz.f64) over ~2e7 squared distances x in [2^-80, 2^20): the
+ * seed the near pairs of ER_PREC_NEAR64 refine by one Newton step, whose
+ * error is the square of this. No counterpart in the reference (FP64 `/`). */
+int er_probe_rcp64_seed(er_ctx* ctx, double* max_rel_err);
 
 /* Library version string. */
 const char* er_version(void);

@@ -441,3 +441,12 @@ def test_batch_comp_equals_single_comp(ctx, mode):
     for u, f, o in zip(ups, fws, outs):
         single = ctx.grid(u, f.dims, precision=er.ER_PREC_COMP)
         assert np.array_equal(o.cpu().numpy(), single)
+
+
+def test_rcp64_seed_error_bound(ctx):
+    """The FP64 near terms of ER_PREC_NEAR64 refine the hardware reciprocal
+    seed by one Newton step, which squares its relative error: the seed must
+    stay below 2^-16 (so a refined reciprocal is within ~2^-32) over the
+    squared distances the near pairs meet."""
+    e0 = ctx.rcp64_seed_error()
+    assert 0.0 < e0 < 2.0 ** -16, e0

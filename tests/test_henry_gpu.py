@@ -182,3 +182,27 @@ def test_henry_batch_errors(ctx):
         ctx.henry_batch([fw, Gone()], 298.0, 100, [1, 2])
     # the context stays usable
     assert ctx.henry_batch([fw], 298.0, 1000, [5])[0][0] == ctx.henry(fw, 298.0, 1000, 5)
+
+
+def test_henry_stage_timing(ctx):
+    """er_ctx_set_timing / er_henry_last_timing: per-stage device times of the
+    last er_henry call, positive and within the call's own duration; timing
+    leaves the result unchanged and is an error while it is off."""
+    import time
+
+    import emptyroom_b200 as er
+    f, P, fw = _fw(ctx, 4, n_atoms=300)
+    ref = ctx.henry(fw, 298.0, 200000, seed=9)
+    ctx.set_timing(True)
+    try:
+        t0 = time.perf_counter()
+        got = ctx.henry(fw, 298.0, 200000, seed=9)
+        wall_ms = (time.perf_counter() - t0) * 1e3
+        t = ctx.henry_timing()
+    finally:
+        ctx.set_timing(False)
+    assert got == ref
+    assert all(v > 0 for v in t.values()), t
+    assert sum(t.values()) <= wall_ms, (t, wall_ms)
+    with pytest.raises(er.ErError, match="timing is off"):
+        ctx.henry_timing()
