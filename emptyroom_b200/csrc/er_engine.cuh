@@ -292,11 +292,17 @@ __device__ __forceinline__ double rcp64_nr(double x) {
     const double e = fma(-x, y, 1.0);
     return fma(y, e, y);
 }
-// acc + the FP64 pair term of a near pair (PREC_NEAR64): r^2 from dx and the
-// shared dy^2 + dz^2, reciprocal by rcp64_nr, the term added by one FMA.
-__device__ __forceinline__ double near_acc64(double acc, double dx, double yz, double c12,
-                                             double c6, double r2min) {
-    const double u = rcp64_nr(fmax(fma(dx, dx, yz), r2min));
+// acc + the FP64 pair term of a near pair (PREC_NEAR64): r^2 = dx^2 + yzc from
+// dx and yzc = dy^2 + dz^2 + min_r^2, formed once per atom and lane, with the
+// reference's clamp r^2 >= min_r^2 (src/computegridsheet.h:77) folded into
+// yzc: both keep r^2 >= min_r^2, and min_r^2 (1e-24 or 1e-32 A^2) lies below
+// the FP64 resolution of r^2 unless r^2 < ~1e-8 A^2, a point within 1e-4 A of
+// an atom, whose energy (> 1e40 K) is capped either way. (The clamp as a
+// separate FP64 max cost 3 % of the 256-framework batch.) Reciprocal by
+// rcp64_nr, the term added by one FMA.
+__device__ __forceinline__ double near_acc64(double acc, double dx, double yzc, double c12,
+                                             double c6) {
+    const double u = rcp64_nr(fma(dx, dx, yzc));
     const double u3 = u * u * u;
     return fma(u3, fma(c12, u3, -c6), acc);
 }
@@ -995,10 +1001,12 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
     if (nrec > 0) recheck_borderline<Pol, PREC>(s, pol, fw, cc, wl, n_sh, win, nrec, rec, L);
     // --- near lists in FP64: exact positions (FP64 images and points relative
     // to the CTA centre) and FP64 (C12, C6). Atom-outer order: one atom's loads
-    // serve up to kNearP of the lane's points, so a pass keeps 2 kNearP FP64
-    // registers of point state.
+    // serve kNearP of the lane's points per pass.
     if (kNear && n_ni + n_ns > 0) {
-        constexpr int kNearP = P < 4 ? P : 4;
+        // lattice lanes take all P points in one pass (their FP32 list state is
+        // dead by now, so the FP64 point state fits the 80 registers); generic
+        // points, with their own y and z each, take passes of 4
+        constexpr int kNearP = Pol::kLattice ? P : (P < 4 ? P : 4);
         double o0, o1, o2;
         cta_centre(s, o0, o1, o2);
 #pragma unroll 1
@@ -1033,16 +1041,16 @@ __device__ __forceinline__ void warp_flush_body(EngineSmem& s, const Pol& pol, c
                 if (Pol::kLattice) {
                     // a lattice lane's points share y and z: dy^2 + dz^2 once per atom
                     const double dy = qy[0] - a.y, dz = qz[0] - a.z;
-                    const double yz = fma(dz, dz, dy * dy);
+                    const double yzc = fma(dz, dz, fma(dy, dy, cc.r2min));
 #pragma unroll
                     for (int p = 0; p < kNearP; ++p)
-                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x, yz, a.c12, a.c6, cc.r2min);
+                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x, yzc, a.c12, a.c6);
                 } else {
 #pragma unroll
                     for (int p = 0; p < kNearP; ++p) {
                         const double dy = qy[p] - a.y, dz = qz[p] - a.z;
-                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x, fma(dz, dz, dy * dy), a.c12,
-                                             a.c6, cc.r2min);
+                        nacc[p] = near_acc64(nacc[p], qx[p] - a.x,
+                                             fma(dz, dz, fma(dy, dy, cc.r2min)), a.c12, a.c6);
                     }
                 }
             }

@@ -368,6 +368,10 @@ struct er_server {
                 cudaGetLastError();
                 status = ER_ERR_CUDA;
             }
+            // a bounded wait that gave up in some kernel of the context since the
+            // last check: the job finishing now is failed (the word is per
+            // context, so a concurrent job's fault may land on this one)
+            if (status == ER_OK && er::take_fault(ctx) != ER_OK) status = ER_ERR_CUDA;
             if (j.job.kind == ER_JOB_HENRY && status == ER_OK)
                 er::henry_finish(*sl.pinned, j.job.n_insertions, j.job.temperature, &j.st.henry);
             if (j.job.kind == ER_JOB_GRID) {
