@@ -146,6 +146,7 @@ SIGNATURES = {
     "er_version": (ctypes.c_char_p, []),
     "er_probe_fp32_rate": (c_int, [c_void_p, c_double, _dp]),
     "er_probe_rcp64_seed": (c_int, [c_void_p, _dp]),
+    "er_selftest_wait_timeout": (c_int, [c_void_p, c_int]),
 }
 
 _lib = None

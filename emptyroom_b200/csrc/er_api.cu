@@ -1172,6 +1172,35 @@ extern "C" int er_probe_rcp64_seed(er_ctx* ctx, double* max_rel_err) {
     return ER_OK;
 }
 
+// One CTA waits, with the engine's bounded wait, for an mbarrier phase that
+// nothing completes (no arrival, no copy); when the wait gives up it raises
+// the fault word of `fault` as the engine's staging waits do.
+__global__ void wait_timeout_kernel(int spins, int* fault) {
+    __shared__ unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool gave_up = !mbar_wait(&bar, 0u, spins);
+    if (__syncthreads_or(gave_up) && threadIdx.x == 0) {
+        atomicExch(fault, 1);
+        mbar_inval(&bar);
+    }
+}
+
+extern "C" int er_selftest_wait_timeout(er_ctx* ctx, int spins) {
+    if (!ctx || spins < 1) return ER_ERR_INVALID;
+    ER_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (int st = take_fault(ctx)) return st;  // an earlier fault is reported first
+    wait_timeout_kernel<<<1, 64, 0, ctx->stream>>>(spins, ctx->fault_dev);
+    ER_CUDA(ctx, cudaGetLastError());
+    ER_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (take_fault(ctx) == ER_OK)
+        return set_error(ctx, ER_ERR_CUDA, "selftest: the bounded wait did not report");
+    return ER_OK;
+}
+
 extern "C" int er_probe_fp32_rate(er_ctx* ctx, double seconds, double* instr_per_s) {
     if (!ctx || !instr_per_s || !(seconds > 0)) return ER_ERR_INVALID;
     ER_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -51,16 +51,17 @@ struct HostBuf {
 // Device scratch of one Widom pipeline (er_henry.cu); one per stream that
 // runs Widom jobs concurrently.
 struct HenryScratch {
-    DevBuf pts, bin, order, tmp, counts, starts, e, nblk, part, res, mask;
+    DevBuf pts, bin, order, tmp, counts, starts, e, nblk, part, res, mask, cell;
     // stage boundaries of the last run (er_ctx_set_timing): start, binned,
     // sorted, energies, reduced; ev[0] == nullptr while timing is off
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     size_t bytes() const {
         return pts.cap + bin.cap + order.cap + tmp.cap + counts.cap + starts.cap + e.cap +
-               nblk.cap + part.cap + res.cap + mask.cap;
+               nblk.cap + part.cap + res.cap + mask.cap + cell.cap;
     }
     void release() {
-        DevBuf* b[] = {&pts, &bin, &order, &tmp, &counts, &starts, &e, &nblk, &part, &res, &mask};
+        DevBuf* b[] = {&pts, &bin, &order, &tmp, &counts, &starts, &e, &nblk, &part, &res, &mask,
+                       &cell};
         for (DevBuf* x : b) x->release();
     }
 };

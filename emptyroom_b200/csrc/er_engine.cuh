@@ -170,9 +170,10 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
 // Waits for the phase of `parity` to complete; false after kMbarSpins polls
 // (a copy that never lands: the caller records the fault instead of hanging).
 constexpr int kMbarSpins = 1 << 22;
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity,
+                                          int spins = kMbarSpins) {
     const unsigned a = smem_u32(bar);
-    for (int i = 0; i < kMbarSpins; ++i) {
+    for (int i = 0; i < spins; ++i) {
         unsigned done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -557,6 +558,27 @@ __device__ __forceinline__ void lattice_inner(EngineSmem& s, const unsigned shor
     int q = 0;
     while (q < n_in) {
         const int qe = kComp ? min(q + kChunk, n_in) : n_in;
+        // eight atoms per iteration (one 128-bit load of their list entries):
+        // more independent chains between the MUFU results (256-framework
+        // batch: 350 -> 342 ms against two atoms per iteration)
+        for (; q + 7 < qe; q += 8) {  // q is a multiple of 8 here (chunk starts are)
+            const uint4 eight = *reinterpret_cast<const uint4*>(wl32 + (q >> 1));
+            atom(eight.x & 0xffffu);
+            atom(eight.x >> 16);
+            atom(eight.y & 0xffffu);
+            atom(eight.y >> 16);
+            atom(eight.z & 0xffffu);
+            atom(eight.z >> 16);
+            atom(eight.w & 0xffffu);
+            atom(eight.w >> 16);
+        }
+        for (; q + 3 < qe; q += 4) {
+            const uint2 four = *reinterpret_cast<const uint2*>(wl32 + (q >> 1));
+            atom(four.x & 0xffffu);
+            atom(four.x >> 16);
+            atom(four.y & 0xffffu);
+            atom(four.y >> 16);
+        }
         for (; q + 1 < qe; q += 2) {  // q is even here: chunks have an even length
             const unsigned two = wl32[q >> 1];
             atom(two & 0xffffu);
@@ -718,20 +740,41 @@ __device__ __forceinline__ int generic_packed_lists(EngineSmem& s, const unsigne
         }
     };
     int q = 0;
+    // the FP32 chunk sums of the inner list fold into FP64 registers, added to
+    // the shared totals once (the Widom kernel has the registers for it)
+    double acc64[2 * M];
+#pragma unroll
+    for (int m = 0; m < 2 * M; ++m) acc64[m] = 0.0;
     while (q < n_in) {
         const int qe = kComp ? min(q + PrecTraits<PREC>::inner_chunk, n_in) : n_in;
-        // two atoms per iteration: eight independent FP32 chains for the
-        // scheduler (the kernel is latency-bound at two CTAs per SM)
+        // four atoms per iteration: sixteen independent FP32 chains for the
+        // scheduler (the kernel is latency-bound at two CTAs per SM); with two
+        // shell atoms per iteration and the register fold, 1.247 -> 1.207 ms
+        // per 1e7 insertions on a config-1 cell
+        for (; q + 3 < qe; q += 4) {
+            inner_atom(wl[q]);
+            inner_atom(wl[q + 1]);
+            inner_atom(wl[q + 2]);
+            inner_atom(wl[q + 3]);
+        }
         for (; q + 1 < qe; q += 2) {
             inner_atom(wl[q]);
             inner_atom(wl[q + 1]);
         }
         if (q < qe) inner_atom(wl[q++]);
-        if (kComp) fold_packed<M>(s, acc2);
+        if (kComp) fold_regs<M>(acc64, acc2);
+    }
+    if (kComp) {
+#pragma unroll
+        for (int p = 0; p < 2 * M; ++p) tot_at(s, p) += acc64[p];
     }
     q = 0;
     while (q < n_sh) {
         const int qe = kComp ? min(q + kAccChunk, n_sh) : n_sh;
+        for (; q + 1 < qe; q += 2) {
+            shell_atom(wl[kMaxCand - 1 - q], q);
+            shell_atom(wl[kMaxCand - 2 - q], q + 1);
+        }
         for (; q < qe; ++q) shell_atom(wl[kMaxCand - 1 - q], q);
         if (kComp) fold_packed<M>(s, acc2);
     }

@@ -61,36 +61,70 @@ __device__ __forceinline__ int bin_key(const double* f, const BinGeom& g) {
            (b[2] & 1);
 }
 
-// Corner test of the pocket mask; the cell lookup follows src/gcmc.cc:155-157.
-__device__ __forceinline__ bool blocked_at(const uint8_t* mask, int nx, int ny, int nz,
-                                           const double* p) {
-    const double dxf = __ddiv_rn(1.0, (double)(nx - 1));
-    const double dyf = __ddiv_rn(1.0, (double)(ny - 1));
-    const double dzf = __ddiv_rn(1.0, (double)(nz - 1));
-    const int i0 = min((int)floor(__ddiv_rn(p[0], dxf)), nx - 2);
-    const int j0 = min((int)floor(__ddiv_rn(p[1], dyf)), ny - 2);
-    const int k0 = min((int)floor(__ddiv_rn(p[2], dzf)), nz - 2);
-    for (int di = 0; di < 2; ++di)
-        for (int dj = 0; dj < 2; ++dj)
-            for (int dk = 0; dk < 2; ++dk) {
-                const size_t idx = (size_t)(k0 + dk) + (size_t)(j0 + dj) * nz +
-                                   (size_t)(i0 + di) * ny * nz;
-                if (mask[idx]) return true;
+// Pocket-mask geometry of a grid of nx x ny x nz points with axes i/(N-1):
+// the spacings 1/(N-1) (FP64, the reference's dx, src/gcmc.cc:155-157) and
+// N - 1, for the cell lookup below.
+struct MaskGeom {
+    int n[3];        // points per axis
+    double d[3];     // 1/(N-1), rounded to nearest as the reference computes it
+    double nm1[3];   // N - 1
+};
+
+// Cell index along one axis: floor(p / d) as src/gcmc.cc:155-157 computes
+// it, clamped to N - 2. p * (N - 1) is within a few ulps of p / d, so their
+// floors can differ only where the quotient lies within ~1e-12 of an integer;
+// there the FP64 division itself decides.
+__device__ __forceinline__ int mask_cell(double p, double d, double nm1, int n) {
+    const double q = p * nm1;
+    int c = (int)floor(q);
+    if (fabs(q - rint(q)) < 1e-6) c = (int)floor(__ddiv_rn(p, d));
+    return min(c, n - 2);
+}
+
+// cell[i, j, k] = 1 when any of the 8 grid points at the corners of the cell
+// (i..i+1, j..j+1, k..k+1) is blocked, for i < nx - 1, j < ny - 1,
+// k < nz - 1: an insertion in the cell is blocked exactly when the
+// reference's lookup of its 8 surrounding grid energies meets a blocked one.
+__global__ void mask_cells_kernel(const uint8_t* __restrict__ mask, MaskGeom mg,
+                                  uint8_t* __restrict__ cell) {
+    const int cx = mg.n[0] - 1, cy = mg.n[1] - 1, cz = mg.n[2] - 1;
+    const size_t total = (size_t)cx * cy * cz;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total;
+         c += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(c % cz);
+        const int j = (int)((c / cz) % cy);
+        const int i = (int)(c / ((size_t)cz * cy));
+        uint8_t b = 0;
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj) {
+                const size_t row = (size_t)(j + dj) * mg.n[2] + (size_t)(i + di) * mg.n[1] * mg.n[2];
+                b |= mask[row + k] | mask[row + k + 1];
             }
-    return false;
+        cell[c] = b ? 1 : 0;
+    }
 }
 
 // Insertion i: its point, the mask test, its bin key and its slot in the bin
 // (the count before it; slots within a bin are in arbitrary order, which the
 // per-bin sort makes ascending).
-__global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g, const uint8_t* __restrict__ mask,
-                                 int mnx, int mny, int mnz, int* __restrict__ key,
-                                 int* __restrict__ slot, int* __restrict__ counts,
-                                 float* __restrict__ energies, int* __restrict__ n_blocked) {
+// The blocked test is one load from the cell mask (mask_cells_kernel).
+__global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g,
+                                 const uint8_t* __restrict__ cell, MaskGeom mg,
+                                 int* __restrict__ key, int* __restrict__ slot,
+                                 int* __restrict__ counts, float* __restrict__ energies,
+                                 int* __restrict__ n_blocked) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double f[3];
         insertion_point(seed, (uint64_t)i, f);
-        if (mask && blocked_at(mask, mnx, mny, mnz, f)) {
+        bool blocked = false;
+        if (cell) {
+            const int ci = mask_cell(f[0], mg.d[0], mg.nm1[0], mg.n[0]);
+            const int cj = mask_cell(f[1], mg.d[1], mg.nm1[1], mg.n[1]);
+            const int ck = mask_cell(f[2], mg.d[2], mg.nm1[2], mg.n[2]);
+            blocked = cell[(size_t)ck + (size_t)cj * (mg.n[2] - 1) +
+                           (size_t)ci * (mg.n[1] - 1) * (mg.n[2] - 1)] != 0;
+        }
+        if (blocked) {
             key[i] = -1;
             energies[i] = INFINITY;
             atomicAdd(n_blocked, 1);
@@ -420,8 +454,24 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
     // overwrites it with the sorted insertion indices
     int* slot = (int*)hs.order.ptr;
     if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[0], st));
-    henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_mask, mnx, mny, mnz,
-                                                   (int*)hs.bin.ptr, slot, counts, E, nblk);
+    MaskGeom mg{};
+    const uint8_t* d_cell = nullptr;
+    if (d_mask) {
+        const int dims[3] = {mnx, mny, mnz};
+        for (int k = 0; k < 3; ++k) {
+            mg.n[k] = dims[k];
+            mg.d[k] = 1.0 / (double)(dims[k] - 1);
+            mg.nm1[k] = (double)(dims[k] - 1);
+        }
+        const size_t nc = (size_t)(mnx - 1) * (mny - 1) * (mnz - 1);
+        if (hs.cell.ensure_on(nc, ctx->pool, st))
+            return set_error(ctx, ER_ERR_NOMEM, "henry: cell mask allocation");
+        const int cb = (int)std::min<size_t>((nc + 255) / 256, (size_t)ctx->num_sms * 16);
+        mask_cells_kernel<<<cb, 256, 0, st>>>(d_mask, mg, (uint8_t*)hs.cell.ptr);
+        d_cell = (const uint8_t*)hs.cell.ptr;
+    }
+    henry_gen_kernel<<<gblocks, gthreads, 0, st>>>(seed, n, g, d_cell, mg, (int*)hs.bin.ptr, slot,
+                                                   counts, E, nblk);
     {
         const int tiles = (g.n_keys + kScanTile - 1) / kScanTile;
         scan_tiles_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum);

@@ -462,6 +462,14 @@ int er_probe_fp32_rate(er_ctx* ctx, double seconds, double* instr_per_s);
  * error is the square of this. No counterpart in the reference (FP64 `/`). */
 int er_probe_rcp64_seed(er_ctx* ctx, double* max_rel_err);
 
+/* Self-test of the kernels' bounded waits: one CTA waits, `spins` polls at
+ * most, for a completion barrier that nothing completes; the wait must give
+ * up, raise the context's fault word and let the host see it (ER_OK then;
+ * ER_ERR_CUDA if it did not report). The context stays usable. The staged
+ * producer (build option ER_BULK=1) waits the same way with 2^22 polls. No
+ * counterpart in the reference. */
+int er_selftest_wait_timeout(er_ctx* ctx, int spins);
+
 /* Library version string. */
 const char* er_version(void);
 

@@ -67,3 +67,19 @@ def test_zero_point_lookup_and_widom_limits(ctx):
         ctx.henry(fw, 298.0, 2**31, seed=0)
     with pytest.raises(er.ErError):
         ctx.henry(fw, float("nan"), 1000, seed=0)
+
+
+def test_bounded_wait_gives_up_and_reports(ctx):
+    """A kernel's bounded wait on a completion barrier that nothing completes
+    gives up, raises the context's fault word, and the host sees it; the
+    context then still computes (a small grid equals the one before)."""
+    import numpy as np
+
+    from emptyroom_b200 import _capi, synth
+    f = synth.make_framework(6, (20.0, 20.0, 20.0), (90, 90, 90), 80)
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    before = ctx.grid(fw, (9, 9, 9))
+    st = _capi.lib().er_selftest_wait_timeout(ctx.handle, 4096)
+    assert st == 0, _capi.lib().er_ctx_last_error(ctx.handle)
+    assert np.array_equal(ctx.grid(fw, (9, 9, 9)), before)
+    fw.release()
