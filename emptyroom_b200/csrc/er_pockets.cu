@@ -7,9 +7,11 @@
 // a POCKET unless a walk over those links returns to it in another unit cell.
 // Here:
 //   1. init      label[p] = p for accessible points, -1 otherwise
-//   2. union     lock-free union-find over the -x, -y, -z neighbours; a root
-//                is always linked to a smaller root, so every component ends
-//                rooted at its smallest linear index
+//   2. union     lock-free union-find over the -x, -y, -z neighbours, first
+//                inside 4 x 8 x 32-point tiles in shared memory, then across
+//                the tile faces in global memory; a root is always linked to
+//                a smaller root, so every component ends rooted at its
+//                smallest linear index
 //   3. compress  label[p] = root
 //   4. number    roots ranked in index order (device-wide scan) -- the
 //                reference's segment numbers, since its flood fill meets each
@@ -83,18 +85,92 @@ __device__ __forceinline__ void cc_unite(int* lab, int a, int b) {
     }
 }
 
-__global__ void cc_union(int* __restrict__ lab, int nx, int ny, int nz) {
+// Tiled labelling: a CTA labels one tile of kTI x kTJ x kTK points (k fastest,
+// so a warp reads 32 consecutive points) by union-find in shared memory, then
+// writes each accessible point's label as the global index of its tile-local
+// root. Local indices order like global ones inside a tile, and a tile-local
+// root is the smallest index of its local component, so every label is <= its
+// point and roots point to themselves: a valid state for cc_unite. The unions
+// across tile faces follow in cc_union_faces, after every tile has written
+// (a face union into a tile that had not yet written could be overwritten).
+// Against one grid-wide union pass with global atomics: 0.38 -> 0.26 ms for
+// the device pocket mask of a 129^3 grid (block_pockets_device, host-timed).
+constexpr int kTK = 32, kTJ = 8, kTI = 4, kTile = kTK * kTJ * kTI;
+
+__device__ __forceinline__ int cc_find_s(const int* sl, int x) {
+    int y = sl[x];
+    while (y != x) {
+        x = y;
+        y = sl[x];
+    }
+    return x;
+}
+
+__device__ __forceinline__ void cc_unite_s(int* sl, int a, int b) {
+    for (;;) {
+        a = cc_find_s(sl, a);
+        b = cc_find_s(sl, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a; a = b; b = t;
+        }
+        const int old = atomicCAS(&sl[a], a, b);
+        if (old == a) return;
+        a = old;
+    }
+}
+
+__global__ void __launch_bounds__(256) cc_union_tiles(int* __restrict__ lab, int nx, int ny,
+                                                      int nz) {
+    __shared__ int sl[kTile];
+    const int tk = (nz + kTK - 1) / kTK, tj = (ny + kTJ - 1) / kTJ;
+    const int k0 = (blockIdx.x % tk) * kTK;
+    const int j0 = ((blockIdx.x / tk) % tj) * kTJ;
+    const int i0 = (blockIdx.x / (tk * tj)) * kTI;
+    const int64_t syz = (int64_t)ny * nz;
+    auto gidx = [&](int q, bool& in) -> int64_t {
+        const int lk = q % kTK, lj = (q / kTK) % kTJ, li = q / (kTK * kTJ);
+        const int i = i0 + li, j = j0 + lj, k = k0 + lk;
+        in = i < nx && j < ny && k < nz;
+        return (int64_t)k + (int64_t)j * nz + (int64_t)i * syz;
+    };
+    for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
+        bool in;
+        const int64_t g = gidx(q, in);
+        sl[q] = (in && lab[g] >= 0) ? q : -1;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
+        if (sl[q] < 0) continue;
+        const int lk = q % kTK, lj = (q / kTK) % kTJ, li = q / (kTK * kTJ);
+        if (lk > 0 && sl[q - 1] >= 0) cc_unite_s(sl, q, q - 1);
+        if (lj > 0 && sl[q - kTK] >= 0) cc_unite_s(sl, q, q - kTK);
+        if (li > 0 && sl[q - kTK * kTJ] >= 0) cc_unite_s(sl, q, q - kTK * kTJ);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
+        if (sl[q] < 0) continue;
+        bool in;
+        const int64_t g = gidx(q, in);
+        lab[g] = (int)gidx(cc_find_s(sl, q), in);
+    }
+}
+
+// Unions across the lower faces of the tiles (global union-find).
+__global__ void cc_union_faces(int* __restrict__ lab, int nx, int ny, int nz) {
     const int64_t n = (int64_t)nx * ny * nz;
     const int64_t syz = (int64_t)ny * nz;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
          p += (int64_t)gridDim.x * blockDim.x) {
-        if (lab[p] < 0) continue;
         const int k = (int)(p % nz);
         const int j = (int)((p / nz) % ny);
         const int i = (int)(p / syz);
-        if (k > 0 && lab[p - 1] >= 0) cc_unite(lab, (int)p, (int)(p - 1));
-        if (j > 0 && lab[p - nz] >= 0) cc_unite(lab, (int)p, (int)(p - nz));
-        if (i > 0 && lab[p - syz] >= 0) cc_unite(lab, (int)p, (int)(p - syz));
+        const bool fk = k > 0 && k % kTK == 0, fj = j > 0 && j % kTJ == 0;
+        const bool fi = i > 0 && i % kTI == 0;
+        if (!(fk || fj || fi) || lab[p] < 0) continue;
+        if (fk && lab[p - 1] >= 0) cc_unite(lab, (int)p, (int)(p - 1));
+        if (fj && lab[p - nz] >= 0) cc_unite(lab, (int)p, (int)(p - nz));
+        if (fi && lab[p - syz] >= 0) cc_unite(lab, (int)p, (int)(p - syz));
     }
 }
 
@@ -344,7 +420,13 @@ static int segment_and_classify(er_ctx* ctx, PocketScratch& ps, cudaStream_t st,
     int* lab = (int*)ps.lab.ptr;
     int* seg = (int*)ps.seg.ptr;
     const int gb = std::max(1, std::min<int>((int)((n + 255) / 256), ctx->num_sms * 16));
-    cc_union<<<gb, 256, 0, st>>>(lab, nx, ny, nz);
+    {
+        const int64_t tiles = (int64_t)((nz + kTK - 1) / kTK) * ((ny + kTJ - 1) / kTJ) *
+                              ((nx + kTI - 1) / kTI);
+        if (tiles > INT32_MAX) return set_error(ctx, ER_ERR_LIMIT, "pockets: grid too large");
+        cc_union_tiles<<<(unsigned)tiles, 256, 0, st>>>(lab, nx, ny, nz);
+        cc_union_faces<<<gb, 256, 0, st>>>(lab, nx, ny, nz);
+    }
     cc_compress<<<gb, 256, 0, st>>>(lab, n);
     const int nblk = (int)((n + kScanItems - 1) / kScanItems);
     // p_misc: block counts (nblk) | block offsets (nblk + 1) | link count | table | list
