@@ -1249,14 +1249,15 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
 
 // ER_BULK=1 (a build option: `make -C emptyroom_b200/csrc clean all cli
 // ER_BULK=1`) selects the producer whose cell-row image ranges arrive in
-// shared memory by bulk copies of the TMA engine (cp.async.bulk, 256 images per stage, two stages in flight, each
-// completing on an mbarrier). Measured on the 256-framework batch it is
-// slower than the default producer (per-thread loads of the same images):
-// 382.8 against 373.6 ms in the default mode, 311.3 against 303.1 ms in
-// ER_PREC_COMP, the Widom energy kernel 1.296 against 1.278 ms per 1e7
-// insertions -- each stage adds a block-wide wait, and the staging state
-// raises the producer's register spills (grid_persistent_kernel<3>: 364 /
-// 1000 bytes of spill stores / loads against 280 / 584).
+// shared memory by bulk copies of the TMA engine (cp.async.bulk, 256 images
+// per stage, two stages in flight, each completing on an mbarrier whose wait
+// is bounded). Measured on the 256-framework batch it is slower than the
+// default producer (per-thread loads of the same images): 382.8 against
+// 373.6 ms in the default mode, 311.3 against 303.1 ms in ER_PREC_COMP, the
+// Widom energy kernel 1.296 against 1.278 ms per 1e7 insertions -- each stage
+// adds a block-wide wait, and the staging state raises the producer's
+// register spills (grid_persistent_kernel<3>: 364 / 1000 bytes of spill
+// stores / loads against 280 / 584).
 #ifndef ER_BULK
 #define ER_BULK 0
 #endif

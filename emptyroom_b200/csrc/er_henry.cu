@@ -97,7 +97,8 @@ __global__ void mask_cells_kernel(const uint8_t* __restrict__ mask, MaskGeom mg,
         uint8_t b = 0;
         for (int di = 0; di < 2; ++di)
             for (int dj = 0; dj < 2; ++dj) {
-                const size_t row = (size_t)(j + dj) * mg.n[2] + (size_t)(i + di) * mg.n[1] * mg.n[2];
+                const size_t row =
+                    (size_t)(j + dj) * mg.n[2] + (size_t)(i + di) * mg.n[1] * mg.n[2];
                 b |= mask[row + k] | mask[row + k + 1];
             }
         cell[c] = b ? 1 : 0;
