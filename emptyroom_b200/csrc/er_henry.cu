@@ -592,7 +592,16 @@ extern "C" int er_ctx_set_timing(er_ctx* ctx, int on) {
     ER_CUDA(ctx, cudaSetDevice(ctx->device));
     HenryScratch& hs = ctx->henry;
     if (on && !hs.ev[0]) {
-        for (cudaEvent_t& e : hs.ev) ER_CUDA(ctx, cudaEventCreate(&e));
+        cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        for (cudaEvent_t& e : ev) {
+            const cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) {
+                for (cudaEvent_t& x : ev)
+                    if (x) cudaEventDestroy(x);
+                return cuda_error(ctx, err, "henry timing: cudaEventCreate");
+            }
+        }
+        for (int k = 0; k < 5; ++k) hs.ev[k] = ev[k];
     } else if (!on && hs.ev[0]) {
         ER_SYNC(ctx, ctx->stream);
         for (cudaEvent_t& e : hs.ev) {

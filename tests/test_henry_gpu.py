@@ -206,3 +206,28 @@ def test_henry_stage_timing(ctx):
     assert sum(t.values()) <= wall_ms, (t, wall_ms)
     with pytest.raises(er.ErError, match="timing is off"):
         ctx.henry_timing()
+
+
+def test_blocked_insertions_match_the_reference_lookup(ctx):
+    """2e6 Philox insertions against a sparse mask on a 23^3 grid: the blocked
+    count equals the reference's lookup (src/gcmc.cc:155-157: cell
+    floor(x / (1/(N-1))) clamped to N-2, any of its 8 corners blocked),
+    evaluated here in numpy on the same points, including the points whose
+    scaled coordinate lies within 1e-6 of a cell plane, where the library
+    decides by the FP64 division itself."""
+    f, P, fw = _fw(ctx, 7, n_atoms=60)
+    N, n, seed = 23, 2_000_000, 17
+    rng = np.random.default_rng(9)
+    mask = (rng.random((N, N, N)) < 0.04).astype(np.uint8)
+    r = ctx.henry(fw, 298.0, n, seed=seed, block_mask=mask)
+    pts = oracle.insertion_points(seed, n)
+    d = 1.0 / (N - 1)
+    cell = np.minimum(np.floor(pts / d).astype(np.int64), N - 2)
+    blocked = np.zeros(n, dtype=bool)
+    for di in (0, 1):
+        for dj in (0, 1):
+            for dk in (0, 1):
+                blocked |= mask[cell[:, 0] + di, cell[:, 1] + dj, cell[:, 2] + dk] != 0
+    q = pts * (N - 1)
+    assert int((np.abs(q - np.rint(q)) < 1e-6).sum()) > 0  # the division path is met
+    assert r["n_blocked"] == int(blocked.sum())
