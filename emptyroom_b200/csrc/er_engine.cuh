@@ -1252,12 +1252,12 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
 // shared memory by bulk copies of the TMA engine (cp.async.bulk, 256 images
 // per stage, two stages in flight, each completing on an mbarrier whose wait
 // is bounded). Measured on the 256-framework batch it is slower than the
-// default producer (per-thread loads of the same images): 382.8 against
-// 373.6 ms in the default mode, 311.3 against 303.1 ms in ER_PREC_COMP, the
-// Widom energy kernel 1.296 against 1.278 ms per 1e7 insertions -- each stage
-// adds a block-wide wait, and the staging state raises the producer's
-// register spills (grid_persistent_kernel<3>: 364 / 1000 bytes of spill
-// stores / loads against 280 / 584).
+// default producer (per-thread loads of the same images): 352.1 against
+// 341.6 ms in the default mode, 305.8 against 297.3 ms in ER_PREC_COMP, a
+// Widom call of 1e7 insertions 1.741 against 1.727 ms -- each stage adds a
+// block-wide wait, and the staging state raises the producer's register
+// spills (grid_persistent_kernel<3>: 364 / 1000 bytes of spill stores / loads
+// against 280 / 584).
 #ifndef ER_BULK
 #define ER_BULK 0
 #endif
