@@ -288,8 +288,12 @@ __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, 
 // 256-framework batch and took 0.8 % longer). x is a squared distance,
 // clamped to >= min_r^2 > 0 by the caller, so the seed is finite and normal.
 __device__ __forceinline__ double rcp64_nr(double x) {
+#if ER_RCP32SEED
+    const double y = (double)rcp_approx((float)x);
+#else
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#endif
     const double e = fma(-x, y, 1.0);
     return fma(y, e, y);
 }
