@@ -70,7 +70,9 @@ struct PrecTraits {
     // near terms to FP64, the rounding of the FP32 partial sums (its error
     // grows with the chunk length times the partial's magnitude) is what is
     // left: 16-atom partials keep every E < -10 K point of the 256-framework
-    // batch within 1e-5 of FP64, 64-atom ones leave 82 of 1.4e8 above it.
+    // batch within 1e-5 of FP64, 64-atom ones leave 82 of 1.4e8 above it;
+    // 32-atom ones were 0.8 % faster but raised the sampled p99 error from
+    // 5.1e-7 to 6.6e-7.
     static constexpr int inner_chunk = PREC == PREC_NEAR64 ? 16 : 64;
 };
 
@@ -285,15 +287,12 @@ __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, 
 // most ~6 x 2^-32 of its own size, far below the 1e-5 relative bound on the
 // energy even where near terms cancel a thousandfold (a third-order step,
 // e0^3, gave the same errors on 71,378 sampled E < -10 K points of the
-// 256-framework batch and took 0.8 % longer). x is a squared distance,
+// 256-framework batch and took 0.8 % longer; a seed from the FP32
+// reciprocal, converted, took 4.7 % longer). x is a squared distance,
 // clamped to >= min_r^2 > 0 by the caller, so the seed is finite and normal.
 __device__ __forceinline__ double rcp64_nr(double x) {
-#if ER_RCP32SEED
-    const double y = (double)rcp_approx((float)x);
-#else
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-#endif
     const double e = fma(-x, y, 1.0);
     return fma(y, e, y);
 }
