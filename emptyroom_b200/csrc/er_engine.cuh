@@ -1273,7 +1273,9 @@ __device__ void process_cta(EngineSmem& s, const Pol& pol, const FwDev& fw,
     }
     __syncthreads();
 #endif
+#if ER_BULK
     unsigned mph = 0;    // phase parity of each staging barrier
+#endif
     bool fault = false;  // a staging wait gave up
     // 3. producer: rows of cells around the CTA box, streamed into shared memory
     const double R = cc.rcm, R2 = R * R;
