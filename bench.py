@@ -450,6 +450,9 @@ def run_ours(args, ws, rank, local, pg):
                  "note": "same batch with every pair term in FP32 (ER_PREC_COMP): faster, "
                          "but outside 1e-5 relative on some E < 0 points"},
     }
+    # the FP64 reciprocal seed the default mode's near pairs refine by one
+    # Newton step (their error is its square)
+    line["rcp64_seed_max_rel_err"] = ctx.rcp64_seed_error()
     cores = os.cpu_count() or 1
     if rank == 0 and ws == 1 and not args.no_errors:
         line["errors"] = {"grids": grid_errors_block(fws, outs, cores)}

@@ -281,9 +281,9 @@ __device__ __forceinline__ double pair64(const Atom64& a, double qx, double qy, 
 }
 // 1/x in FP64 for the near pairs of PREC_NEAR64: one Newton step
 // y = y0 (1 + e), e = 1 - x y0, from the hardware seed y0 =
-// rcp.approx.ftz.f64(x), whose relative error e0 is below 2^-16 (measured by
-// er_probe_rcp64_seed, asserted by the tests), leaves a relative error of
-// order e0^2 < 2^-32 plus two FP64 roundings. A near term then carries at
+// rcp.approx.ftz.f64(x), whose relative error e0 is below 2^-16 (asserted by
+// the tests; er_probe_rcp64_seed measures 9.9e-7, about 2^-20), leaves a
+// relative error of order e0^2 < 2^-32 plus two FP64 roundings. A near term then carries at
 // most ~6 x 2^-32 of its own size, far below the 1e-5 relative bound on the
 // energy even where near terms cancel a thousandfold (a third-order step,
 // e0^3, gave the same errors on 71,378 sampled E < -10 K points of the
