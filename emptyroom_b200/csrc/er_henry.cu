@@ -641,7 +641,43 @@ extern "C" int er_henry_last_timing(er_ctx* ctx, er_henry_timing* out) {
 namespace er {
 namespace {
 
-constexpr int kHenryPipes = 3;
+// Up to 6 pipelines: on 64 config-4 frameworks (1e7 insertions, 80^3 pocket
+// grids) 2, 3, 4 and 6 took 136.0, 133.8, 132.6 and 130.7 ms. Each holds its
+// own scratch, so the count is also cut to what half the free device memory
+// holds (henry_pipe_count).
+constexpr int kHenryPipes = 6;
+
+// Device bytes one pipeline holds for a job: 40 per insertion (Cartesian
+// FP64 point, bin key, order, scan scratch, FP32 energy), 24 per blocking-grid
+// point (FP32 grid, mask, pocket labels and segments), plus the bin tables.
+size_t henry_pipe_bytes(int64_t n_ins, const int bd[3]) {
+    return 40 * (size_t)n_ins + 24 * (size_t)bd[0] * bd[1] * bd[2] + ((size_t)64 << 20);
+}
+
+int henry_pipe_count(er_ctx* ctx, int n, int64_t n_ins, const int bd[3]) {
+    int np = std::min(n, kHenryPipes);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    // memory the pool keeps for reuse, and the pipelines' own scratch, count
+    // as free: a new job grows into them first
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
+            cudaSuccess &&
+        cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+        free_b += (size_t)(reserved - used);
+    else
+        cudaGetLastError();
+    for (int p = 0; p < np && p < (int)ctx->pipes.size(); ++p) {
+        const HenryPipe& P = *ctx->pipes[p];
+        free_b += P.hs.bytes() + P.grid.cap + P.mask.cap;
+    }
+    const size_t fit = free_b / 2 / henry_pipe_bytes(n_ins, bd);
+    return (int)std::max<size_t>(1, std::min<size_t>(np, fit));
+}
 
 int henry_one(er_ctx* ctx, HenryPipe& P, const FwRecord& fw, double temperature, int64_t n_ins,
               uint64_t seed, const int bd[3], er_henry_result* out, int* n_pockets) {
@@ -697,7 +733,7 @@ extern "C" int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temp
         if (!(fr[k] = find_fw(ctx, fw_ids[k])))
             return set_error(ctx, ER_ERR_NOT_FOUND,
                              "henry batch: unknown framework id (entry " + std::to_string(k) + ")");
-    const int np = std::min(n, kHenryPipes);
+    const int np = henry_pipe_count(ctx, n, n_insertions, bd);
     while ((int)ctx->pipes.size() < np) {
         HenryPipe* p = new HenryPipe();
         if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||

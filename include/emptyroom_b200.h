@@ -198,10 +198,12 @@ int er_henry(er_ctx* ctx, int fw_id, double temperature, int64_t n_ins, uint64_t
  * the FP32 energy grid of block_nx x block_ny x block_nz points (as er_grid
  * with default flags), its pocket mask (as er_block_pockets_device, pocketblocking.cc:
  * 126-391) and er_henry of fw_ids[k] with seed seeds[k] and that mask; with
- * all three dims 0, er_henry alone. The frameworks run on up to three
+ * all three dims 0, er_henry alone. The frameworks run on up to six
  * concurrent pipelines (a stream, scratch and a host thread each, kept by the
- * context), so that one framework's grid, labelling, binning and host round
- * trips overlap another's energy kernel. Each results[k] (and n_pockets[k],
+ * context; fewer when half the free device memory holds fewer pipelines'
+ * scratch, about 40 bytes per insertion and 24 per blocking-grid point each),
+ * so that one framework's grid, labelling, binning and host round trips
+ * overlap another's energy kernel. Each results[k] (and n_pockets[k],
  * when n_pockets is not NULL) equals the single calls' bit for bit. On an
  * error the remaining entries are not run. */
 int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
