@@ -969,8 +969,10 @@ def case_refgpu(ctx, args):
 def run_case(args):
     """Single-kernel and analysis cases: `config3` runs the 4096-atom triclinic
     cell on a dims^3 grid (one er_grid launch per step); `widom` runs er_henry
-    with --insertions points on a config-1 cell; `precision` the precision
-    sweep; `refgpu` this library beside the reference's own GPU writegrid."""
+    with --insertions points on a config-1 cell; `widom_batch` er_henry_batch
+    over --widom-frameworks config-4 cells (pocket grid, device mask and
+    --insertions points each); `precision` the precision sweep; `refgpu` this
+    library beside the reference's own GPU writegrid."""
     import torch
 
     import emptyroom_b200 as er
@@ -1007,6 +1009,22 @@ def run_case(args):
                           "precision": args.precision, "ms": t * 1e3, "pairs": pairs,
                           "pair_terms_per_s": pairs / t,
                           "pairs_per_point": pairs / float(np.prod(dims))}))
+    elif args.case == "widom_batch":
+        fws = synth.config4(args.widom_frameworks)
+        ups = ctx.upload_many([(f.particles(), f.t_matrix, f.rep, f.rc2) for f in fws])
+        dims = fws[0].dims
+        times = []
+        for k in range(args.warmup + args.steps):
+            seeds = [k * len(ups) + j for j in range(len(ups))]
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            res, _ = ctx.henry_batch(ups, 298.0, args.insertions, seeds, block_dims=dims)
+            if k >= args.warmup:
+                times.append(time.perf_counter() - t0)
+        t = sum(times) / len(times)
+        n_ins = args.insertions * len(ups)
+        print(json.dumps({"case": "widom_batch", "frameworks": len(ups), "dims": list(dims),
+                          "insertions": n_ins, "ms": t * 1e3, "insertions_per_s": n_ins / t}))
     else:
         f = synth.make_framework(0, (25.8, 25.8, 25.8), (90, 90, 90), 424, probe="Xe")
         fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
@@ -1032,7 +1050,7 @@ def main():
     ap.add_argument("--no-errors", action="store_true",
                     help="skip the oracle comparison of the grids and K_H")
     ap.add_argument("--case", default="batch",
-                    choices=["batch", "config3", "widom", "precision", "refgpu"])
+                    choices=["batch", "config3", "widom", "widom_batch", "precision", "refgpu"])
     ap.add_argument("--dims", type=int, default=256)
     ap.add_argument("--atoms", type=int, default=4096)
     ap.add_argument("--tree", default="/tmp/er_tree")

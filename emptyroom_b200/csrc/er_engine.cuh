@@ -886,8 +886,12 @@ static __device__ __noinline__ void recheck_borderline(EngineSmem& s, const Pol&
     const float rc2f = cc.rc2f;
     const bool all = nrec > kRec;
     const int nq = all ? n_sh : nrec;
+    // ascending list positions either way (the latest record sits in the low
+    // bits), so the corrections of a point add up in one order whichever
+    // points share its thread: an energy depends only on its warp's and CTA's
+    // point sets, not on where in the warp the point sits
     for (int r = 0; r < nq; ++r) {
-        const int q = all ? r : (int)((rec >> (10 * r)) & 1023u);
+        const int q = all ? r : (int)((rec >> (10 * (nq - 1 - r))) & 1023u);
         const unsigned off = wl[kMaxCand - 1 - q];
         const Cand& cd = s.cand[off >> 5];
         const float ss = Pol::kLattice ? ss_lattice(L.py[0], L.pz[0], cd.ay, cd.az) : 0.f;

@@ -5,8 +5,10 @@
 //   1. gen     insertion i -> Philox4x32-10 point (stream `seed`), pocket-mask
 //              test, spatial bin key (bins of ~32 expected points, 2x2x2 bricks)
 //   2. scan    bin counts -> bin starts
-//   3. scatter insertion indices into their bins; 4. sort each bin ascending
-//      (so the layout, and with it every FP32 rounding, is deterministic)
+//   3. scatter insertion indices into their bins; 4. place each sorted
+//      position's point, then order the bins that straddle a warp boundary by
+//      insertion index (so every warp's point set, and with it every FP32
+//      rounding, is deterministic)
 //   5. energy  the shared LJ engine over 2048 (1024 for runs below 1e6)
 //              sorted points per CTA
 //   6. reduce  FP64 log-sum-exp of exp(-E/T) and E exp(-E/T) in insertion
@@ -106,15 +108,18 @@ __global__ void mask_cells_kernel(const uint8_t* __restrict__ mask, MaskGeom mg,
 }
 
 // Insertion i: its point, the mask test, its bin key and its slot in the bin
-// (the count before it; slots within a bin are in arbitrary order, which the
-// per-bin sort makes ascending).
+// (the count before it; slots within a bin are in arbitrary order, which is
+// made ascending where a bin straddles a warp boundary).
 // The blocked test is one load from the cell mask (mask_cells_kernel).
 __global__ void henry_gen_kernel(uint64_t seed, int n, BinGeom g,
                                  const uint8_t* __restrict__ cell, MaskGeom mg,
                                  int* __restrict__ key, int* __restrict__ slot,
                                  int* __restrict__ counts, float* __restrict__ energies,
                                  int* __restrict__ n_blocked) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // 64-bit stride: near the 2^31 - 4097 limit i + stride leaves int
+    for (long long ii = blockIdx.x * (long long)blockDim.x + threadIdx.x; ii < n;
+         ii += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)ii;
         double f[3];
         insertion_point(seed, (uint64_t)i, f);
         bool blocked = false;
@@ -259,12 +264,30 @@ int scan_exclusive(er_ctx* ctx, const int* in, int n, int* out, int* tile_sums,
     return ER_OK;
 }
 
+// Four insertions per thread (16-byte loads of key and slot): their four
+// bin-start lookups are in flight together (the kernel waits on those
+// dependent loads; one insertion per thread took 0.108 ms per 1e7).
 __global__ void henry_scatter_kernel(const int* __restrict__ key, const int* __restrict__ slot,
                                      int n, const int* __restrict__ starts,
                                      int* __restrict__ tmp) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int k = key[i];
-        if (k >= 0) tmp[starts[k] + slot[i]] = i;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; 4 * g < n;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int i0 = (int)(4 * g);
+        if (i0 + 4 <= n) {
+            const int4 k = *reinterpret_cast<const int4*>(key + i0);
+            const int4 q = *reinterpret_cast<const int4*>(slot + i0);
+            const int s0 = k.x >= 0 ? starts[k.x] : 0, s1 = k.y >= 0 ? starts[k.y] : 0;
+            const int s2 = k.z >= 0 ? starts[k.z] : 0, s3 = k.w >= 0 ? starts[k.w] : 0;
+            if (k.x >= 0) tmp[s0 + q.x] = i0;
+            if (k.y >= 0) tmp[s1 + q.y] = i0 + 1;
+            if (k.z >= 0) tmp[s2 + q.z] = i0 + 2;
+            if (k.w >= 0) tmp[s3 + q.w] = i0 + 3;
+        } else {
+            for (int i = i0; i < n; ++i) {
+                const int k = key[i];
+                if (k >= 0) tmp[starts[k] + slot[i]] = i;
+            }
+        }
     }
 }
 
@@ -273,37 +296,79 @@ struct Frame {
     double r[9];
 };
 
-// One warp per bin: rank of each entry among its bin's entries -> ascending
-// order (the bin's entries compared 32 at a time through shuffles); the
-// insertion point itself (recomputed from its Philox counter) is written in the
-// same sorted order as its Cartesian position in frame r (the engine's own
+// The energy kernel's result for an insertion depends only on the set of
+// insertions in its warp (warp_pts consecutive sorted positions) and in its
+// CTA, not on their order there: every sum is per point, over lists built from
+// the warp and CTA boxes, and the exact cutoff corrections add up in list
+// order. So a bin inside one warp's positions keeps the order of its atomic
+// slots (which varies from run to run), and only a bin that straddles a warp
+// boundary (one in eight at ~4 P points per bin) is put in ascending insertion
+// order, which fixes the set on either side of the boundary. Sorting every bin
+// (a warp per bin) took 0.33 ms per 1e7 insertions with the scatter; ordering
+// only the straddling bins in that kernel 0.25 ms.
+//
+// The insertion point (recomputed from its Philox counter) is written at its
+// position as its Cartesian position in frame r (the engine's own
 // frac_to_cart, so the bits are those the engine would compute), which the
 // energy kernel reads coalesced.
-__global__ void henry_sort_bins_kernel(const int* __restrict__ starts, int n_keys,
-                                       const int* __restrict__ tmp, uint64_t seed, Frame fr,
-                                       int* __restrict__ order, double* __restrict__ pts_sorted) {
+__device__ __forceinline__ void put_point(uint64_t seed, const Frame& fr, int v, double* dst) {
+    double f[3], x, y, z;
+    insertion_point(seed, (uint64_t)v, f);
+    frac_to_cart(fr.r, f[0], f[1], f[2], x, y, z);
+    dst[0] = x;
+    dst[1] = y;
+    dst[2] = z;
+}
+
+// Every sorted position p < n_valid, one thread each: the insertion the
+// scatter put there and its point.
+__global__ void henry_place_kernel(const int* __restrict__ n_valid, const int* __restrict__ tmp,
+                                   uint64_t seed, Frame fr, int* __restrict__ order,
+                                   double* __restrict__ pts) {
+    const long long nv = *n_valid;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < nv;
+         p += (long long)gridDim.x * blockDim.x) {
+        const int v = tmp[p];
+        order[p] = v;
+        put_point(seed, fr, v, pts + 3 * p);
+    }
+}
+
+// One warp per warp boundary m * warp_pts (m >= 1) below n_valid, after
+// henry_place_kernel: the bin holding that position (binary search of the bin
+// starts); when the boundary cuts it and is the first boundary to do so, the
+// warp rewrites the bin in ascending insertion order (each entry's rank among
+// the bin's entries, compared 32 at a time through shuffles).
+__global__ void henry_order_straddling_kernel(const int* __restrict__ starts, int n_keys,
+                                              int warp_pts, const int* __restrict__ tmp,
+                                              uint64_t seed, Frame fr, int* __restrict__ order,
+                                              double* __restrict__ pts) {
     const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n_keys; b += warps) {
-        const int s = starts[b], L = starts[b + 1] - s;
-        for (int q0 = 0; q0 < L; q0 += 32) {
-            const int q = q0 + lane;
-            const int v = q < L ? tmp[s + q] : INT_MAX;
-            int rank = 0;
-            for (int r0 = 0; r0 < L; r0 += 32) {
-                const int u = r0 + lane < L ? tmp[s + r0 + lane] : INT_MAX;
+    const long long m = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) + 1;
+    const long long qb = m * warp_pts;
+    if (qb >= starts[n_keys]) return;
+    const int q = (int)qb;
+    // the last bin b with starts[b] <= q: q lies in [starts[b], starts[b + 1])
+    int lo = 0, hi = n_keys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    const int s = starts[lo], L = starts[lo + 1] - s;
+    if (s == q || q - warp_pts > s) return;  // not cut here, or cut first by an earlier boundary
+    for (int q0 = 0; q0 < L; q0 += 32) {
+        const int i = q0 + lane;
+        const int v = i < L ? tmp[s + i] : INT_MAX;
+        int rank = 0;
+        for (int r0 = 0; r0 < L; r0 += 32) {
+            const int u = r0 + lane < L ? tmp[s + r0 + lane] : INT_MAX;
 #pragma unroll
-                for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, u, k) < v;
-            }
-            if (q < L) {
-                order[s + rank] = v;
-                double f[3], x, y, z;
-                insertion_point(seed, (uint64_t)v, f);
-                frac_to_cart(fr.r, f[0], f[1], f[2], x, y, z);
-                pts_sorted[3 * (size_t)(s + rank)] = x;
-                pts_sorted[3 * (size_t)(s + rank) + 1] = y;
-                pts_sorted[3 * (size_t)(s + rank) + 2] = z;
-            }
+            for (int k = 0; k < 32; ++k) rank += __shfl_sync(0xffffffffu, u, k) < v;
+        }
+        if (i < L) {
+            order[s + rank] = v;
+            put_point(seed, fr, v, pts + 3 * (size_t)(s + rank));
         }
     }
 }
@@ -347,19 +412,23 @@ __global__ void __launch_bounds__(256) henry_reduce_kernel(const float* __restri
                                                            Lse* __restrict__ part) {
     __shared__ Lse sm[256];
     const int lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
-    Lse acc{-INFINITY, 0.0, 0.0};
+    // two passes over this thread's entries: the largest exponent, then the
+    // weights exp(x - m), which do not wait for one another (with a running
+    // maximum every exp waited for the previous one). x is the rounded product
+    // in both passes (__dmul_rn: no FMA contraction into x - m), so the largest
+    // entry's weight is exactly 1 also for capped energies, where |x| ~ 1e27.
+    double m = -INFINITY;
     for (int i = lo + threadIdx.x; i < hi; i += 256) {
         const float ef = E[i];
-        if (isinf(ef)) continue;  // blocked insertion: weight 0
-        const double e = (double)ef;
-        const double x = e * neg_inv_t;
-        if (x > acc.m) {
-            const double f = exp(acc.m - x);
-            acc.s = acc.s * f + 1.0;
-            acc.se = acc.se * f + e;
-            acc.m = x;
-        } else {
-            const double w = exp(x - acc.m);
+        if (!isinf(ef)) m = fmax(m, __dmul_rn((double)ef, neg_inv_t));  // blocked: weight 0
+    }
+    Lse acc{m, 0.0, 0.0};
+    if (m > -INFINITY) {
+        for (int i = lo + threadIdx.x; i < hi; i += 256) {
+            const float ef = E[i];
+            if (isinf(ef)) continue;
+            const double e = (double)ef;
+            const double w = exp(__dmul_rn(e, neg_inv_t) - m);
             acc.s += w;
             acc.se += e * w;
         }
@@ -480,19 +549,26 @@ int henry_enqueue(er_ctx* ctx, const FwRecord& fw, double temperature, int n, ui
         scan_apply_kernel<<<tiles, kScanThreads, 0, st>>>(counts, g.n_keys, tsum, starts);
     }
     if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[1], st));
-    // one thread per insertion for the scatter and one warp per bin for the sort
-    // (more blocks in flight hide their dependent loads: 1.77 -> 1.75 ms per
-    // 1e7 insertions against grid-stride loops over 16 CTAs per SM)
-    const int sblocks = (int)std::min<int64_t>((n + gthreads - 1) / gthreads, 1 << 20);
-    const int bblocks = (int)std::min<int64_t>(((int64_t)g.n_keys + 7) / 8, 1 << 20);
+    // a thread per four insertions for the scatter and a thread per position
+    // for the placement, up to 2^20 CTAs each (more blocks in flight hide their
+    // dependent loads; key and slot are pool allocations, 16-byte aligned);
+    // a warp per warp boundary for the straddling bins
+    const int sblocks = (int)std::min<int64_t>(((int64_t)n + 4 * gthreads - 1) / (4 * gthreads),
+                                               1 << 20);
+    const int pblocks = (int)std::min<int64_t>(((int64_t)n + gthreads - 1) / gthreads, 1 << 20);
     henry_scatter_kernel<<<sblocks, gthreads, 0, st>>>((const int*)hs.bin.ptr, slot, n, starts,
                                                        (int*)hs.tmp.ptr);
     Frame fr;
     for (int k = 0; k < 9; ++k) fr.r[k] = fw.dev.r[k];
-    henry_sort_bins_kernel<<<bblocks, 256, 0, st>>>(starts, g.n_keys,
-                                                              (const int*)hs.tmp.ptr, seed, fr,
-                                                              (int*)hs.order.ptr,
-                                                              (double*)hs.pts.ptr);
+    henry_place_kernel<<<pblocks, gthreads, 0, st>>>(starts + g.n_keys, (const int*)hs.tmp.ptr,
+                                                      seed, fr, (int*)hs.order.ptr,
+                                                      (double*)hs.pts.ptr);
+    const int warp_pts = 32 * henry_points_per_thread(n);
+    const int64_t n_bounds = ((int64_t)n - 1) / warp_pts;  // boundaries below n
+    if (n_bounds > 0)
+        henry_order_straddling_kernel<<<(int)((n_bounds + 7) / 8), 256, 0, st>>>(
+            starts, g.n_keys, warp_pts, (const int*)hs.tmp.ptr, seed, fr, (int*)hs.order.ptr,
+            (double*)hs.pts.ptr);
     ER_CUDA(ctx, cudaGetLastError());
     if (hs.ev[0]) ER_CUDA(ctx, cudaEventRecord(hs.ev[2], st));
     PointTask task;

@@ -64,26 +64,25 @@ __global__ void __launch_bounds__(256) partial_kernel(const float* __restrict__ 
     __shared__ Stats sm[256];
     const int64_t lo = (int64_t)blockIdx.x * chunk;
     const int64_t hi = lo + chunk < n ? lo + chunk : n;
+    // two passes over this thread's entries, as er_henry's reduction: the
+    // counts and the largest exponent, then the weights exp(x - m)
     Stats acc{-INFINITY, 0.0, 0.0, 0.0, 0.0};
     for (int64_t i = lo + threadIdx.x; i < hi; i += 256) {
         const float ef = E[i];
         if (ef == INFINITY) {  // +inf (a blocked insertion) has weight 0
             acc.n_inf += 1.0;
-            continue;
-        }
-        if (isnan(ef) || ef == -INFINITY) {  // no defined weight
+        } else if (isnan(ef) || ef == -INFINITY) {  // no defined weight
             acc.n_bad += 1.0;
-            continue;
-        }
-        const double e = (double)ef;
-        const double x = -e / T;
-        if (x > acc.m) {
-            const double f = exp(acc.m - x);
-            acc.s = acc.s * f + 1.0;
-            acc.se = acc.se * f + e;
-            acc.m = x;
         } else {
-            const double w = exp(x - acc.m);
+            acc.m = fmax(acc.m, -(double)ef / T);
+        }
+    }
+    if (acc.m > -INFINITY) {
+        for (int64_t i = lo + threadIdx.x; i < hi; i += 256) {
+            const float ef = E[i];
+            if (isinf(ef) || isnan(ef)) continue;
+            const double e = (double)ef;
+            const double w = exp(-e / T - acc.m);
             acc.s += w;
             acc.se += e * w;
         }

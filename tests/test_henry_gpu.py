@@ -62,6 +62,24 @@ def test_henry_deterministic(ctx):
     assert c["sum_w"] != a["sum_w"]
 
 
+def test_henry_energies_independent_of_bin_order(ctx):
+    """A bin inside one warp's positions keeps the run-dependent order of its
+    atomic slots; only each warp's set of insertions is fixed. Repeated calls
+    (both points-per-thread paths) and six pipelines running the same
+    framework and seed at once, their atomics racing one another, must give
+    the same bits."""
+    f = synth.config1(0)
+    fw = ctx.upload(f.particles(), f.t_matrix, f.rep, f.rc2)
+    for n in (200_000, 2_000_000):
+        ref = ctx.henry(fw, 298.0, n, seed=21, want_energies=True)
+        for _ in range(2):
+            r = ctx.henry(fw, 298.0, n, seed=21, want_energies=True)
+            assert np.array_equal(r["energies"], ref["energies"])
+        got, _ = ctx.henry_batch([fw] * 6, 298.0, n, [21] * 6)
+        for g in got:
+            assert g["sum_w"] == ref["sum_w"] and g["mean_energy"] == ref["mean_energy"]
+
+
 def test_henry_with_block_mask(ctx):
     f, P, fw = _fw(ctx, 5, n_atoms=300)
     T = 298.0
