@@ -212,8 +212,10 @@ int er_henry_batch(er_ctx* ctx, const int* fw_ids, int n, double temperature,
 
 /* Device time (ms) of each stage of the last er_henry call on ctx, taken with
  * CUDA events on the context stream while timing is on (er_ctx_set_timing,
- * off by default): Philox points, mask test and bin counts; the bin sort; the
- * Lennard-Jones energy kernel; the FP64 log-sum-exp reduction. The reference
+ * off by default): Philox points, mask test and bin counts; the bin layout
+ * (scatter into bins, placement of each point, ordering of the bins that
+ * straddle a warp boundary); the Lennard-Jones energy kernel; the FP64
+ * log-sum-exp reduction. The reference
  * times only the whole run ("Simulation time", src/henry.cu:150-153).
  * er_henry_batch, the server and er_henry_stats_noalloc record nothing. */
 typedef struct {
