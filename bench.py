@@ -562,7 +562,7 @@ def run_widom(ctx, args, fp32_rate, errors=True):
         grid_pairs += c
         mean_pairs.append(c / float(np.prod(dims)))
         ins_pairs += mean_pairs[-1] * n_ins
-    # the Widom pipeline of one framework alone (Philox points, bin sort,
+    # the Widom pipeline of one framework alone (Philox points, bin layout,
     # energy kernel, FP64 log-sum-exp), device-timed on the library's stream,
     # with the energy kernel's own time from the library's stage events
     ctx.grid_device(ups[0], dims, g.data_ptr())

@@ -421,7 +421,8 @@ struct PointPolicy {
         ok = pos < nv;
         return ok ? pos : min(base, nv - 1);  // a finite stand-in, never stored
     }
-    // Cartesian position (frame r), stored in sorted order by the bin sort
+    // Cartesian position (frame r), stored at its bin-order position by the
+    // placement pass
     __device__ __forceinline__ bool cart(const double*, int w, int lane, int p, double& x,
                                          double& y, double& z) const {
         bool ok;

@@ -10,7 +10,7 @@
 //      insertion index (so every warp's point set, and with it every FP32
 //      rounding, is deterministic)
 //   5. energy  the shared LJ engine over 2048 (1024 for runs below 1e6)
-//              sorted points per CTA
+//              points per CTA, in bin order
 //   6. reduce  FP64 log-sum-exp of exp(-E/T) and E exp(-E/T) in insertion
 //              order with a fixed tree: (m, s, se) with sum w = s e^m.
 #include <math.h>
