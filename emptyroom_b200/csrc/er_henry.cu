@@ -305,7 +305,8 @@ struct Frame {
 // boundary (one in eight at ~4 P points per bin) is put in ascending insertion
 // order, which fixes the set on either side of the boundary. Sorting every bin
 // (a warp per bin) took 0.33 ms per 1e7 insertions with the scatter; ordering
-// only the straddling bins in that kernel 0.25 ms.
+// only the straddling bins in that kernel 0.25 ms; a thread per position for
+// the placement and a warp per boundary for the straddling bins 0.24 ms.
 //
 // The insertion point (recomputed from its Philox counter) is written at its
 // position as its Cartesian position in frame r (the engine's own
