@@ -80,3 +80,14 @@ def grid_errors(e_gpu, e_ref, scale=None, loose=False):
     cap = e_ref >= 1e30
     out["cap_ok"] = bool(np.all(e_gpu[cap] == np.float32(1e30)))
     return out
+
+
+def rotated_cell(t, seed):
+    """t rotated by a seeded proper rotation (a cell matrix that is not upper
+    triangular; same lattice up to rotation, so the same energies)."""
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
+    q = q * np.sign(np.diag(r))
+    if np.linalg.det(q) < 0:
+        q[:, 0] = -q[:, 0]
+    return q @ np.asarray(t, dtype=np.float64).reshape(3, 3)

@@ -6,7 +6,7 @@ import pytest
 
 import emptyroom_b200 as er
 import oracle
-from conftest import golden, grid_errors
+from conftest import golden, grid_errors, rotated_cell
 from emptyroom_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -276,15 +276,7 @@ def test_near64_is_more_accurate_than_comp(ctx):
     assert np.all(np.abs(e64 - ref)[neg] <= 2e-6 * np.abs(ref[neg]) + 2e-4)
 
 
-def _rotated(t, seed):
-    """t rotated by a seeded proper rotation (a cell matrix that is not upper
-    triangular; same lattice up to rotation, so the same energies)."""
-    rng = np.random.default_rng(seed)
-    q, r = np.linalg.qr(rng.normal(size=(3, 3)))
-    q = q * np.sign(np.diag(r))
-    if np.linalg.det(q) < 0:
-        q[:, 0] = -q[:, 0]
-    return q @ np.asarray(t, dtype=np.float64).reshape(3, 3)
+_rotated = rotated_cell
 
 
 @pytest.mark.parametrize("flags", [0, er.ER_TILE_P8])

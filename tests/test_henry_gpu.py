@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import grid_errors
+from conftest import grid_errors, rotated_cell
 from emptyroom_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -106,6 +106,31 @@ def test_henry_triclinic_masked_matches_oracle(ctx, n_ins):
         pts = np.array([oracle.insertion_point(33, int(i)) for i in ok])
         S = oracle.points_abs(P, f.t_matrix, f.rep, f.rc2, pts, 1e-16)
         st = grid_errors(r["energies"][ok], o["energies"][ok], S)
+        assert st["neg_ok"] and st["pos_ok"] and st["cap_ok"], st
+
+
+@pytest.mark.parametrize("n_ins", [40000, 1_050_000])
+def test_henry_rotated_cell_matches_oracle(ctx, n_ins):
+    """A cell matrix that is not upper triangular: the insertion points go to
+    Cartesian coordinates through the positioning frame, the exact cutoff
+    decisions through the cell matrix itself. K_H within 1e-6 and (the
+    smaller run) the first 3000 energies within the grid tolerances of the
+    FP64 oracle on the same rotated matrix."""
+    f = synth.make_framework(160, (16.0, 19.0, 17.5), (75, 105, 98), 140, probe="Kr")
+    P = f.particles()
+    t = rotated_cell(f.t_matrix, 3)
+    assert abs(t[1, 0]) > 1e-3 and abs(t[2, 0]) > 1e-3
+    fw = ctx.upload(P, t, f.rep, f.rc2)
+    T = 298.0
+    want = n_ins < 100000
+    r = ctx.henry(fw, T, n_ins, seed=44, want_energies=want)
+    o = oracle.henry_cells(P, t, f.rep, f.rc2, T, 44, n_ins, want_energies=want)
+    kh_o = _kh(o["sum_w"], n_ins, T)
+    assert abs(r["kh_mol_m3_pa"] - kh_o) <= KH_RTOL * kh_o
+    if want:
+        pts = np.array([oracle.insertion_point(44, i) for i in range(3000)])
+        S = oracle.points_abs(P, t, f.rep, f.rc2, pts, 1e-16)
+        st = grid_errors(r["energies"][:3000], o["energies"][:3000], S)
         assert st["neg_ok"] and st["pos_ok"] and st["cap_ok"], st
 
 
