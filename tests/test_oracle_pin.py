@@ -146,15 +146,24 @@ def test_cell_list_sum_equals_image_loop(k):
     assert np.all(np.abs(g - g0) <= 1e-13 * S)
 
 
-def test_cell_list_henry_equals_image_loop():
+@pytest.mark.parametrize("cell", ["cubic", "triclinic", "rotated"])
+def test_cell_list_henry_equals_image_loop(cell):
+    """The cell-list Widom oracle (the reference for the GPU Widom tests on
+    triclinic and rotated cells) equals the image loop."""
+    from conftest import rotated_cell
     from emptyroom_b200 import synth
-    f = synth.make_framework(63, (14.0, 15.0, 13.0), (90, 90, 90), 120, probe="Xe")
+    if cell == "cubic":
+        f = synth.make_framework(63, (14.0, 15.0, 13.0), (90, 90, 90), 120, probe="Xe")
+    elif cell == "triclinic":
+        f = synth.make_framework(77, (14.0, 16.0, 18.0), (85.0, 100.0, 115.0), 90, probe="CH4")
+    else:
+        f = synth.make_framework(160, (16.0, 19.0, 17.5), (75, 105, 98), 140, probe="Kr")
+    t = rotated_cell(f.t_matrix, 3) if cell == "rotated" else f.t_matrix
     P = f.particles()
     mask = (np.random.default_rng(2).random((9, 8, 10)) < 0.05).astype(np.uint8)
     for m in (None, mask):
-        a = oracle.henry(P, f.t_matrix, f.rep, f.rc2, 298.0, 9, 3000, mask=m,
-                         want_energies=True)
-        b = oracle.henry_cells(P, f.t_matrix, f.rep, f.rc2, 298.0, 9, 3000, mask=m,
+        a = oracle.henry(P, t, f.rep, f.rc2, 298.0, 9, 3000, mask=m, want_energies=True)
+        b = oracle.henry_cells(P, t, f.rep, f.rc2, 298.0, 9, 3000, mask=m,
                                want_energies=True)
         assert a["n_blocked"] == b["n_blocked"]
         assert abs(a["sum_w"] - b["sum_w"]) <= 1e-12 * a["sum_w"]
